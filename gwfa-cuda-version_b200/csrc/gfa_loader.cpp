@@ -1,0 +1,659 @@
+// gfa_loader.cpp — GFA input side of the GWFA path: parse S/L lines (and FASTA-as-graph),
+// finalize the bidirected graph, extract the topologically ordered subgraph reachable from the
+// start vertex, and convert it to a gwf_graph_t.
+//
+// Behaviour follows the reference loader so that vertex numbering, sequences and arcs match
+// `gwf-test -p` byte for byte:
+//   parsing            gfa-io.c:115-220 (S), gfa-io.c:222-324 (L), gfa-io.c:326-427 (FASTA, read)
+//   finalize           gfa-base.c:455-466 (no_seg, arc sort/index, semi arcs, symmetric arcs,
+//                      arc lengths, cleanup), gfa-base.c:235-371
+//   subgraph order     gfa-sub.c:41-272 (Kahn's algorithm with an ordered queue keyed by
+//                      (in-degree left, distance, vertex) and the orphan / forced rules)
+//   conversion         main.cu:294-345 (gwf_gfa2gwf), dump main.cu:354-359
+// The containers are this file's own (std::vector, std::set, std::unordered_map).
+#include <zlib.h>
+#include <algorithm>
+#include <climits>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <set>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/gwfa.h"
+#include "gwfa_internal.h"
+
+namespace {
+
+struct Seg {
+	std::string name;
+	int32_t len = 0;
+	bool has_seq = false;
+	std::string seq;
+	bool del = false;
+};
+
+struct Arc {
+	uint64_t v_lv = 0; // vertex << 32 | lv
+	uint32_t w = 0;
+	int32_t ov = 0, ow = 0;
+	uint64_t link_id = 0;
+	bool del = false, comp = false;
+	uint32_t head() const { return (uint32_t)(v_lv >> 32); }
+};
+
+struct Gfa {
+	std::vector<Seg> seg;
+	std::unordered_map<std::string, uint32_t> names;
+	std::vector<Arc> arc;
+	std::vector<uint64_t> idx; // per vertex: first << 32 | n
+
+	uint32_t add_seg(const std::string &name)
+	{
+		auto it = names.find(name);
+		if (it != names.end()) return it->second;
+		uint32_t id = (uint32_t)seg.size();
+		seg.emplace_back();
+		seg.back().name = name;
+		names.emplace(name, id);
+		return id;
+	}
+	uint32_t n_vtx() const { return (uint32_t)seg.size() << 1; }
+	uint32_t arc_n(uint32_t v) const { return v < idx.size() ? (uint32_t)idx[v] : 0; }
+	uint32_t arc_off(uint32_t v) const { return v < idx.size() ? (uint32_t)(idx[v] >> 32) : 0; }
+	void add_arc(uint32_t v, uint32_t w, int32_t ov, int32_t ow, int64_t link_id, bool comp)
+	{
+		Arc a;
+		a.v_lv = (uint64_t)v << 32;
+		a.w = w, a.ov = ov, a.ow = ow;
+		a.link_id = link_id >= 0 ? (uint64_t)link_id : (uint64_t)arc.size();
+		a.comp = comp;
+		arc.push_back(a);
+	}
+	void arc_sort()
+	{
+		std::stable_sort(arc.begin(), arc.end(),
+		                 [](const Arc &x, const Arc &y) { return x.v_lv < y.v_lv; });
+	}
+	void arc_index() // gfa-base.c:214-229
+	{
+		idx.assign((size_t)seg.size() * 2, 0);
+		size_t n = arc.size(), last = 0;
+		for (size_t i = 1; i <= n; ++i)
+			if (i == n || arc[i - 1].head() != arc[i].head()) {
+				uint32_t h = arc[i - 1].head();
+				if (h < idx.size()) idx[h] = (uint64_t)last << 32 | (i - last);
+				last = i;
+			}
+	}
+};
+
+// ---------------------------------------------------------------- tag helpers
+// Finds "XY:T:value" among tab-separated optional fields; returns pointer to value or null.
+const char *find_tag(const std::vector<std::string> &tags, const char *key, char type)
+{
+	for (const auto &t : tags)
+		if (t.size() >= 5 && t[0] == key[0] && t[1] == key[1] && t[2] == ':' && t[3] == type &&
+		    t[4] == ':')
+			return t.c_str() + 5;
+	return nullptr;
+}
+
+void split_tabs(const std::string &line, std::vector<std::string> &out)
+{
+	out.clear();
+	size_t st = 0;
+	for (size_t i = 0; i <= line.size(); ++i)
+		if (i == line.size() || line[i] == '\t') {
+			out.emplace_back(line, st, i - st);
+			st = i + 1;
+		}
+}
+
+bool is_tag(const std::string &t)
+{
+	return t.size() >= 5 && t[2] == ':' && t[4] == ':' &&
+	       (t[3] == 'A' || t[3] == 'i' || t[3] == 'f' || t[3] == 'Z' || t[3] == 'B');
+}
+
+// gfa-io.c:115-220
+int parse_S(Gfa &g, const std::string &line)
+{
+	std::vector<std::string> f;
+	split_tabs(line, f); // f[0] == "S"
+	if (f.size() < 3) return -1;
+	const std::string &name = f[1], &sq = f[2];
+	std::vector<std::string> tags;
+	for (size_t i = 3; i < f.size(); ++i)
+		if (is_tag(f[i])) tags.push_back(f[i]);
+	int32_t LN = -1;
+	if (const char *p = find_tag(tags, "LN", 'i')) LN = (int32_t)strtol(p, nullptr, 10);
+	bool has_seq = !(sq.size() > 0 && sq[0] == '*');
+	int32_t len = 0;
+	if (!has_seq) {
+		if (LN >= 0) len = LN;
+	} else
+		len = (int32_t)strlen(sq.c_str());
+	uint32_t sid = g.add_seg(name);
+	Seg &s = g.seg[sid];
+	s.len = len;
+	s.has_seq = has_seq;
+	s.seq = has_seq ? std::string(sq.c_str()) : std::string();
+	return 0;
+}
+
+// gfa-io.c:222-324
+int parse_L(Gfa &g, const std::string &line)
+{
+	std::vector<std::string> f;
+	split_tabs(line, f);
+	if (f.size() < 5) return -1;
+	const std::string &segv = f[1], &segw = f[3];
+	if (f[2].empty() || (f[2][0] != '+' && f[2][0] != '-')) return -2;
+	if (f[4].empty() || (f[4][0] != '+' && f[4][0] != '-')) return -2;
+	int oriv = f[2][0] != '+', oriw = f[4][0] != '+';
+	int32_t ov = 0, ow = 0;
+	std::vector<std::string> tags;
+	if (f.size() >= 6) {
+		const char *q = f[5].c_str();
+		bool ok = false;
+		if (*q == '*') {
+			ov = ow = 0, ok = true;
+		} else if (*q == ':') {
+			ov = INT32_MAX;
+			ow = isdigit((unsigned char)q[1]) ? (int32_t)strtol(q + 1, nullptr, 10) : INT32_MAX;
+			ok = true;
+		} else if (isdigit((unsigned char)*q)) {
+			char *r;
+			long first = strtol(q, &r, 10);
+			if (isupper((unsigned char)*r)) { // CIGAR
+				ov = ow = 0;
+				const char *p = q;
+				do {
+					char *e;
+					long l = strtol(p, &e, 10);
+					p = e;
+					if (*p == 'M' || *p == 'D' || *p == 'N') ov += (int32_t)l;
+					if (*p == 'M' || *p == 'I' || *p == 'S') ow += (int32_t)l;
+					++p;
+				} while (isdigit((unsigned char)*p));
+				ok = true;
+			} else if (*r == ':') {
+				ov = (int32_t)first;
+				ow = isdigit((unsigned char)r[1]) ? (int32_t)strtol(r + 1, nullptr, 10) : INT32_MAX;
+				ok = true;
+			}
+		}
+		if (!ok) ov = ow = 0; // unparsable overlap: treated like a missing field (gfa-io.c:277)
+		for (size_t i = 6; i < f.size(); ++i)
+			if (is_tag(f[i])) tags.push_back(f[i]);
+	}
+	uint32_t v = g.add_seg(segv) << 1 | (uint32_t)oriv;
+	uint32_t w = g.add_seg(segw) << 1 | (uint32_t)oriw;
+	g.add_arc(v, w, ov, ow, -1, false);
+	if (const char *p = find_tag(tags, "L1", 'i'))
+		if (ov != INT32_MAX) {
+			int32_t l1 = (int32_t)strtol(p, nullptr, 10);
+			Seg &s = g.seg[v >> 1];
+			if (ov + l1 > s.len) s.len = ov + l1;
+		}
+	if (const char *p = find_tag(tags, "L2", 'i'))
+		if (ow != INT32_MAX) {
+			int32_t l2 = (int32_t)strtol(p, nullptr, 10);
+			Seg &s = g.seg[w >> 1];
+			if (ow + l2 > s.len) s.len = ow + l2;
+		}
+	return 0;
+}
+
+// ---------------------------------------------------------------- finalize (gfa-base.c)
+void fix_no_seg(Gfa &g)
+{
+	for (auto &s : g.seg)
+		if (s.len == 0) s.del = true;
+}
+
+void fix_semi_arc(Gfa &g) // gfa-base.c:269-301
+{
+	uint32_t nvt = g.n_vtx();
+	for (uint32_t v = 0; v < nvt; ++v) {
+		uint32_t nv = g.arc_n(v), ofs = g.arc_off(v);
+		for (uint32_t i = 0; i < nv; ++i) {
+			Arc &avi = g.arc[ofs + i];
+			if (avi.del || (avi.ow != INT32_MAX && avi.ov != INT32_MAX)) continue;
+			uint32_t w = avi.w ^ 1;
+			uint32_t nw = g.arc_n(w), ow_ = g.arc_off(w);
+			int c = 0, jv = -1;
+			bool multi = false;
+			for (uint32_t j = 0; j < nw; ++j)
+				if (!g.arc[ow_ + j].del && g.arc[ow_ + j].w == (v ^ 1)) ++c, jv = (int)j;
+			if (c == 1) {
+				const Arc &awj = g.arc[ow_ + jv];
+				if (avi.ov != INT32_MAX && awj.ow != INT32_MAX && avi.ov != awj.ow) multi = true;
+				if (avi.ow != INT32_MAX && awj.ov != INT32_MAX && avi.ow != awj.ov) multi = true;
+			}
+			if (c == 1 && !multi) {
+				const Arc &awj = g.arc[ow_ + jv];
+				if (awj.ov != INT32_MAX) avi.ow = awj.ov;
+				if (awj.ow != INT32_MAX) avi.ov = awj.ow;
+			} else
+				avi.del = true;
+		}
+	}
+}
+
+void fix_symm_add(Gfa &g) // gfa-base.c:303-338
+{
+	uint32_t nvt = g.n_vtx();
+	size_t n0 = g.arc.size();
+	for (uint32_t v = 0; v < nvt; ++v) {
+		uint32_t nv = g.arc_n(v), ofs = g.arc_off(v);
+		for (uint32_t i = 0; i < nv; ++i) {
+			Arc avi = g.arc[ofs + i];
+			if (avi.del || avi.comp) continue;
+			uint32_t nw = g.arc_n(avi.w ^ 1), ow_ = g.arc_off(avi.w ^ 1), j;
+			for (j = 0; j < nw; ++j) {
+				Arc &awj = g.arc[ow_ + j];
+				if (awj.del || awj.comp) continue;
+				if (awj.w == (v ^ 1) && awj.ov == avi.ow && awj.ow == avi.ov) {
+					awj.comp = true;
+					awj.link_id = avi.link_id;
+					break;
+				}
+			}
+			if (j == nw) g.add_arc(avi.w ^ 1, v ^ 1, avi.ow, avi.ov, (int64_t)avi.link_id, true);
+		}
+	}
+	if (g.arc.size() > n0) {
+		g.arc_sort();
+		g.arc_index();
+	}
+}
+
+void fix_arc_len(Gfa &g) // gfa-base.c:249-267
+{
+	for (auto &a : g.arc) {
+		uint32_t v = a.head(), w = a.w;
+		Seg &sv = g.seg[v >> 1];
+		if (!sv.del && sv.len < a.ov) a.ov = sv.len;
+		if (sv.del || g.seg[w >> 1].del)
+			a.del = true;
+		else
+			a.v_lv |= (uint32_t)(sv.len - a.ov);
+	}
+}
+
+void cleanup(Gfa &g) // gfa-base.c:340-371
+{
+	std::vector<Arc> keep;
+	keep.reserve(g.arc.size());
+	for (const auto &a : g.arc)
+		if (!a.del && !g.seg[a.head() >> 1].del && !g.seg[a.w >> 1].del) keep.push_back(a);
+	g.arc.swap(keep);
+	bool sorted = true;
+	for (size_t e = 1; e < g.arc.size(); ++e)
+		if (g.arc[e - 1].v_lv > g.arc[e].v_lv) {
+			sorted = false;
+			break;
+		}
+	if (!sorted) g.arc_sort();
+	g.arc_index();
+}
+
+void finalize(Gfa &g) // gfa-base.c:455-466
+{
+	fix_no_seg(g);
+	g.arc_sort();
+	g.arc_index();
+	fix_semi_arc(g);
+	fix_symm_add(g);
+	fix_arc_len(g);
+	cleanup(g);
+}
+
+// ---------------------------------------------------------------- reader (gfa-io.c:354-427)
+struct LineSource {
+	gzFile fp = nullptr;
+	const char *mem = nullptr;
+	int64_t mem_len = 0, mem_pos = 0;
+	std::vector<char> buf;
+	int64_t bpos = 0, blen = 0;
+	bool eof = false;
+
+	bool getc_(int &c)
+	{
+		if (mem) {
+			if (mem_pos >= mem_len) return false;
+			c = (unsigned char)mem[mem_pos++];
+			return true;
+		}
+		if (bpos >= blen) {
+			if (eof) return false;
+			if (buf.empty()) buf.resize(1 << 16);
+			int r = gzread(fp, buf.data(), (unsigned)buf.size());
+			if (r <= 0) {
+				eof = true;
+				return false;
+			}
+			blen = r, bpos = 0;
+		}
+		c = (unsigned char)buf[bpos++];
+		return true;
+	}
+	bool getline(std::string &s)
+	{
+		s.clear();
+		int c;
+		bool any = false;
+		while (getc_(c)) {
+			any = true;
+			if (c == '\n') break;
+			s.push_back((char)c);
+		}
+		if (!s.empty() && s.back() == '\r') s.pop_back();
+		return any;
+	}
+};
+
+bool read_gfa(LineSource &src, Gfa &g)
+{
+	std::string s, fa_seq;
+	bool is_fa = false;
+	int64_t fa_seg = -1;
+	auto flush_fa = [&]() {
+		if (fa_seg >= 0) {
+			Seg &sg = g.seg[(size_t)fa_seg];
+			sg.seq = fa_seq, sg.has_seq = true, sg.len = (int32_t)fa_seq.size();
+		}
+	};
+	while (src.getline(s)) {
+		if (!s.empty() && s[0] == '>') {
+			is_fa = true;
+			flush_fa();
+			char nb[32];
+			snprintf(nb, sizeof nb, "s%u", (unsigned)g.seg.size() + 1);
+			fa_seg = g.add_seg(nb);
+			fa_seq.clear();
+		} else if (is_fa) {
+			if (s.size() >= 3 && s[1] == '\t') {
+				flush_fa();
+				fa_seg = -1, is_fa = false;
+			} else
+				fa_seq += s;
+		}
+		if (is_fa) continue;
+		if (s.size() < 3 || s[1] != '\t') continue;
+		int ret = 0;
+		if (s[0] == 'S') ret = parse_S(g, s);
+		else if (s[0] == 'L') ret = parse_L(g, s);
+		(void)ret; // the reference reports and skips invalid lines
+	}
+	if (is_fa) flush_fa();
+	finalize(g);
+	return true;
+}
+
+// ---------------------------------------------------------------- subgraph (gfa-sub.c:41-272)
+struct TNode {
+	uint64_t xnd;
+	uint32_t v;
+	uint32_t in_tree; // reused as the output index after extraction
+	bool forced;
+};
+inline uint32_t tn_n(const TNode *p) { return (uint32_t)(p->xnd << 1 >> 33); }
+struct TCmp {
+	bool operator()(const TNode *a, const TNode *b) const
+	{
+		return a->xnd < b->xnd || (a->xnd == b->xnd && a->v < b->v);
+	}
+};
+
+struct Sub {
+	std::vector<uint32_t> v;   // oriented GFA vertex of output vertex j
+	std::vector<int32_t> off, n;
+	std::vector<uint64_t> a;   // new target << 32 | arc index in g.arc
+};
+
+void sub_from(const Gfa &g, uint32_t v0, int32_t max_dist, Sub &sub)
+{
+	std::unordered_map<uint32_t, TNode *> h;
+	std::set<TNode *, TCmp> tree;
+	std::vector<TNode *> L, owned;
+	int32_t orphan_inv = 0;
+	auto gen = [&](uint32_t v, uint32_t d) {
+		TNode *p = new TNode;
+		owned.push_back(p);
+		p->v = v, p->in_tree = 1, p->forced = false;
+		p->xnd = 1ULL << 63 | (uint64_t)g.arc_n(v ^ 1) << 32 | d;
+		return p;
+	};
+	auto get = [&](uint32_t v) -> TNode * {
+		auto it = h.find(v);
+		return it == h.end() ? nullptr : it->second;
+	};
+	TNode *p0 = gen(v0, 0);
+	h[v0] = p0;
+	tree.insert(p0);
+	while (!tree.empty()) {
+		TNode *q = nullptr;
+		TNode *r = *tree.begin();
+		if (orphan_inv) {
+			for (auto it = tree.begin(); it != tree.end(); ++it) {
+				TNode *c = get((*it)->v ^ 1);
+				if (c && !c->in_tree) {
+					--orphan_inv;
+					q = *it;
+					tree.erase(it);
+					break;
+				}
+			}
+		} else if (tn_n(r) > 0) {
+			uint32_t rv = r->v ^ 1, nv = g.arc_n(rv), ofs = g.arc_off(rv), i;
+			for (i = 0; i < nv; ++i) {
+				const Arc &avi = g.arc[ofs + i];
+				TNode *k1 = get(avi.w ^ 1), *k2 = get(avi.w);
+				if ((!k1 && k2 && !k2->in_tree) || (!k2 && k1 && !k1->in_tree)) continue;
+				break;
+			}
+			if (i < nv) {
+				std::vector<TNode *> all(tree.begin(), tree.end());
+				tree.clear();
+				for (TNode *x : all) x->xnd &= ~(1ULL << 63);
+				for (TNode *x : all) tree.insert(x);
+			}
+		}
+		if (!q) {
+			q = *tree.begin();
+			tree.erase(tree.begin());
+		}
+		q->forced = (tn_n(q) > 0 || q->xnd >> 63 == 0);
+		q->in_tree = 0;
+		L.push_back(q);
+		if (TNode *c = get(q->v ^ 1))
+			if (c->in_tree) ++orphan_inv;
+		uint32_t d = (uint32_t)q->xnd;
+		uint32_t nv = g.arc_n(q->v), ofs = g.arc_off(q->v);
+		for (uint32_t i = 0; i < nv; ++i) {
+			const Arc &avi = g.arc[ofs + i];
+			int32_t dt = (int32_t)(d + (uint32_t)g.seg[avi.w >> 1].len);
+			if (max_dist > 0 && dt > max_dist) continue;
+			TNode *c = get(avi.w ^ 1);
+			if (c && !c->in_tree && !c->forced) continue;
+			TNode *p = get(avi.w);
+			if (!p) {
+				p = gen(avi.w, (uint32_t)dt);
+				h[avi.w] = p;
+			} else {
+				if (!p->in_tree) continue;
+				tree.erase(p);
+				if ((uint32_t)dt < (uint32_t)p->xnd) p->xnd = p->xnd >> 32 << 32 | (uint32_t)dt;
+			}
+			if (tn_n(p) > 0) p->xnd -= 1ULL << 32;
+			tree.insert(p);
+		}
+	}
+	for (size_t j = 0; j < L.size(); ++j) L[j]->in_tree = (uint32_t)j;
+	sub.v.resize(L.size());
+	sub.off.resize(L.size());
+	sub.n.resize(L.size());
+	sub.a.clear();
+	for (size_t j = 0; j < L.size(); ++j) {
+		size_t o0 = sub.a.size();
+		uint32_t nv = g.arc_n(L[j]->v), ofs = g.arc_off(L[j]->v);
+		for (uint32_t i = 0; i < nv; ++i) {
+			TNode *t = get(g.arc[ofs + i].w);
+			if (!t) continue;
+			sub.a.push_back((uint64_t)t->in_tree << 32 | (uint64_t)(ofs + i));
+		}
+		sub.v[j] = L[j]->v;
+		sub.off[j] = (int32_t)o0;
+		sub.n[j] = (int32_t)(sub.a.size() - o0);
+		std::sort(sub.a.begin() + (long)o0, sub.a.end());
+	}
+	for (TNode *p : owned) delete p;
+}
+
+// IUPAC complement, upper and lower case; every other byte maps to itself (U -> A).
+unsigned char comp_base(unsigned char c)
+{
+	static unsigned char t[256];
+	static bool init = false;
+	if (!init) {
+		for (int i = 0; i < 256; ++i) t[i] = (unsigned char)i;
+		const char *pairs[] = {"AT", "CG", "RY", "KM", "BV", "DH"};
+		for (const char *p : pairs) {
+			t[(unsigned char)p[0]] = (unsigned char)p[1], t[(unsigned char)p[1]] = (unsigned char)p[0];
+			t[(unsigned char)tolower(p[0])] = (unsigned char)tolower(p[1]);
+			t[(unsigned char)tolower(p[1])] = (unsigned char)tolower(p[0]);
+		}
+		t[(unsigned char)'U'] = 'A', t[(unsigned char)'u'] = 'a';
+		init = true;
+	}
+	return t[c];
+}
+
+gwf_graph_t *to_gwf(const Gfa &gfa, uint32_t v0) // main.cu:294-345
+{
+	Sub sub;
+	sub_from(gfa, v0, 1 << 30, sub);
+	gwf_graph_t *g = (gwf_graph_t *)calloc(1, sizeof(gwf_graph_t));
+	g->n_vtx = (uint32_t)sub.v.size();
+	g->n_arc = (uint32_t)sub.a.size();
+	g->len = (uint32_t *)malloc(sizeof(uint32_t) * (g->n_vtx ? g->n_vtx : 1));
+	g->src = (uint32_t *)malloc(sizeof(uint32_t) * (g->n_vtx ? g->n_vtx : 1));
+	g->seq = (char **)calloc(g->n_vtx ? g->n_vtx : 1, sizeof(char *));
+	g->arc = (gwf_arc_t *)calloc(g->n_arc ? g->n_arc : 1, sizeof(gwf_arc_t));
+	bool bad = false;
+	uint32_t k = 0;
+	for (uint32_t i = 0; i < g->n_vtx; ++i) {
+		uint32_t v = sub.v[i];
+		const Seg &s = gfa.seg[v >> 1];
+		uint32_t len = (uint32_t)s.len;
+		g->len[i] = len;
+		g->src[i] = v;
+		g->seq[i] = (char *)malloc(len + 1);
+		if (!s.has_seq || s.seq.size() < len) bad = true;
+		for (uint32_t j = 0; j < len; ++j) {
+			unsigned char c;
+			if (v & 1) {
+				size_t p = (size_t)len - j - 1;
+				c = p < s.seq.size() ? comp_base((unsigned char)s.seq[p]) : 'N';
+			} else
+				c = j < s.seq.size() ? (unsigned char)s.seq[j] : 'N';
+			g->seq[i][j] = (char)c;
+		}
+		g->seq[i][len] = 0;
+		for (int32_t l = 0; l < sub.n[i]; ++l) {
+			uint64_t a = sub.a[(size_t)(sub.off[i] + l)];
+			g->arc[k].a = (uint64_t)i << 32 | (a >> 32);
+			g->arc[k].o = gfa.arc[(uint32_t)a].ow;
+			++k;
+		}
+	}
+	if (bad) gwf_set_error("GFA segment without a sequence (or shorter than LN) on the walk; 'N' used");
+	return g;
+}
+
+gwf_graph_t *load(LineSource &src, const char *start_seg)
+{
+	Gfa gfa;
+	read_gfa(src, gfa);
+	if (gfa.seg.empty()) {
+		gwf_set_error("GFA has no segments");
+		return nullptr;
+	}
+	uint32_t v0 = 0;
+	if (start_seg) {
+		auto it = gfa.names.find(start_seg);
+		if (it == gfa.names.end()) {
+			gwf_set_error("start segment not found");
+			return nullptr;
+		}
+		v0 = it->second << 1;
+	}
+	return to_gwf(gfa, v0);
+}
+
+} // namespace
+
+extern "C" gwf_graph_t *gwf_gfa_load(const char *path, const char *start_seg)
+{
+	LineSource src;
+	src.fp = path && strcmp(path, "-") ? gzopen(path, "r") : gzdopen(0, "r");
+	if (!src.fp) {
+		gwf_set_error("cannot open GFA file");
+		return nullptr;
+	}
+	gwf_graph_t *g = load(src, start_seg);
+	gzclose(src.fp);
+	return g;
+}
+
+extern "C" gwf_graph_t *gwf_gfa_load_mem(const char *text, int64_t len, const char *start_seg)
+{
+	if (!text || len < 0) {
+		gwf_set_error("null GFA text");
+		return nullptr;
+	}
+	LineSource src;
+	src.mem = text, src.mem_len = len;
+	return load(src, start_seg);
+}
+
+extern "C" void gwf_graph_free(gwf_graph_t *g)
+{
+	if (!g) return;
+	gwf_cleanup(g);
+	for (uint32_t i = 0; i < g->n_vtx; ++i) free(g->seq[i]);
+	free(g->len), free(g->src), free(g->seq), free(g->arc);
+	free(g);
+}
+
+extern "C" int64_t gwf_graph_dump(const gwf_graph_t *g, char *buf, int64_t cap)
+{
+	std::string out;
+	char tmp[96];
+	for (uint32_t i = 0; i < g->n_vtx; ++i) {
+		out += "S\t";
+		snprintf(tmp, sizeof tmp, "%d", (int)i);
+		out += tmp;
+		out += '\t';
+		out += g->seq[i];
+		snprintf(tmp, sizeof tmp, "\tLN:i:%d\n", (int)g->len[i]);
+		out += tmp;
+	}
+	for (uint32_t i = 0; i < g->n_arc; ++i) {
+		snprintf(tmp, sizeof tmp, "L\t%d\t+\t%d\t+\t%dM\n", (int)(uint32_t)(g->arc[i].a >> 32),
+		         (int)(uint32_t)g->arc[i].a, g->arc[i].o);
+		out += tmp;
+	}
+	if (buf && cap > 0) {
+		int64_t n = (int64_t)out.size() < cap ? (int64_t)out.size() : cap;
+		memcpy(buf, out.data(), (size_t)n);
+		if (n < cap) buf[n] = 0;
+	}
+	return (int64_t)out.size();
+}

@@ -1,0 +1,514 @@
+// gwf_kernels.cuh — the alignment kernel (plain and persistent forms) and the read packer.
+// See gwf_device.cuh for the algorithm outline and the reference lines each phase restates.
+#pragma once
+#include "gwf_device.cuh"
+
+namespace gwfb {
+
+struct KParams {
+	DevGraph g;
+	DevReads r;
+	const int32_t *order;   // read index per queue position (cost-ordered for persistent)
+	int32_t n_order;
+	int32_t *head;          // persistent: next queue position
+	uint8_t *ws;            // warp arenas
+	int64_t slot_bytes;     // persistent: bytes per warp arena
+	const int64_t *slot_off;// plain: arena byte offset per queue position
+	int32_t level;          // arena size class (retry level)
+	int32_t dens_milli;     // graph density for arena sizing
+	int32_t ql_cap;         // persistent: arenas sized for this read length
+	int32_t flags;          // bit 0: exact start (no reference start-state quirk)
+	int32_t *dist;
+	int32_t *status;
+	int32_t *retry_list;    // reads that overflowed their arena
+	int32_t *retry_n;
+	int32_t *steps_out;     // optional per-read score steps
+	int64_t *w_out;         // optional per-read sum of wavefront sizes
+};
+
+// Aligns read r with one warp. All control flow is warp-uniform.
+__device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *wsb, const Caps &c)
+{
+	const int lane = threadIdx.x & 31;
+	const DevGraph &g = p.g;
+	const WsOff o = ws_layout(c);
+	uint64_t *const h = (uint64_t *)(wsb + o.h);
+	uint64_t *const a_vd = (uint64_t *)(wsb + o.a_vd);
+	int32_t *const a_k = (int32_t *)(wsb + o.a_k);
+	uint64_t *const x_vd = (uint64_t *)(wsb + o.x_vd);
+	int32_t *const x_k = (int32_t *)(wsb + o.x_k);
+	uint64_t *const ba_vd = (uint64_t *)(wsb + o.ba_vd);
+	int32_t *const ba_k = (int32_t *)(wsb + o.ba_k);
+	uint64_t *e_vd = (uint64_t *)(wsb + o.w0_vd);
+	int32_t *e_k = (int32_t *)(wsb + o.w0_k);
+	uint64_t *f_vd = (uint64_t *)(wsb + o.w1_vd);
+	int32_t *f_k = (int32_t *)(wsb + o.w1_k);
+	uint64_t *const n_vd = (uint64_t *)(wsb + o.n_vd);
+	int32_t *const n_k = (int32_t *)(wsb + o.n_k);
+	uint64_t *const tb = (uint64_t *)(wsb + o.tb);
+	uint64_t *const ta = (uint64_t *)(wsb + o.ta);
+	uint64_t *const ilo = (uint64_t *)(wsb + o.i0_lo);
+	uint64_t *const ihi = (uint64_t *)(wsb + o.i0_hi);
+	uint64_t *const clo = (uint64_t *)(wsb + o.i1_lo);
+	uint64_t *const chi = (uint64_t *)(wsb + o.i1_hi);
+
+	ReadCtx rc;
+	rc.ql = p.r.ql[r];
+	rc.v1 = p.r.v1;
+	rc.qpk = p.r.pk + p.r.pk_off[r];
+	rc.qraw = p.r.raw + p.r.raw_off[r];
+	rc.packed = g.pure && p.r.pure[r];
+	rc.quirk = !(p.flags & 1);
+	const int32_t ql = rc.ql, v1 = rc.v1;
+	const int32_t v0 = p.r.v0[r];
+
+	int32_t dist = -1, st = ST_OK, steps = 0;
+	int64_t W = 0;
+	if (ql <= 0 || v0 < 0 || (uint32_t)v0 >= g.n_vtx || (v1 >= 0 && (uint32_t)v1 >= g.n_vtx)) {
+		if (lane == 0) p.dist[r] = -1, p.status[r] = ST_BAD_INPUT;
+		return;
+	}
+
+	// clear the arrival set (16-byte stores; h is 16-byte aligned, c.h is a power of two >= 256)
+	{
+		uint4 *h4 = (uint4 *)h;
+		const uint4 z = make_uint4(0, 0, 0, 0);
+		for (int32_t i = lane; i < c.h / 2; i += 32) h4[i] = z;
+	}
+	if (lane == 0) a_vd[0] = gen_vd((uint32_t)v0, 0), a_k[0] = -1; // gwf-ed.cu:1303-1308
+	__syncwarp();
+	const uint32_t hmask = (uint32_t)c.h - 1;
+	const int32_t hlimit = c.h - c.h / 4;
+	int32_t n_a = 1, n_i = 0, n_keys = 0;
+
+	for (int32_t s = 0;; ++s) {
+		if (s >= c.max_steps) {
+			st = ST_CAPACITY;
+			break;
+		}
+		++steps;
+		W += n_a;
+		bool found = false, ovf = false;
+
+		// ---- phase 1: extend every diagonal; collect vertex-end (and, for v1 >= 0,
+		// query-end) states into the first wave (gwf-ed.cu:902-910, 965-984)
+		int32_t n_e = 0;
+		for (int32_t base = 0; base < n_a; base += 32) {
+			const int32_t j = base + lane;
+			bool toE = false;
+			uint64_t vd = 0;
+			int32_t k = 0;
+			if (j < n_a) {
+				vd = a_vd[j];
+				k = a_k[j];
+				const uint32_t v = vd_v(vd);
+				const int32_t d = vd_d(vd), vl = (int32_t)__ldg(g.len + v);
+				k = ext(g, rc, v, d, k, vl);
+				a_k[j] = k;
+				const bool vend = k == vl - 1, qend = d + k == ql - 1;
+				if (qend) {
+					if (v1 < 0 || ((int32_t)v == v1 && vend)) found = true;
+					else toE = true;
+				} else if (vend)
+					toE = true;
+			}
+			const uint32_t m = __ballot_sync(FULL, toE);
+			const int32_t pos = n_e + __popc(m & lanemask_lt());
+			if (toE && pos < c.w) e_vd[pos] = vd, e_k[pos] = k;
+			n_e += __popc(m);
+		}
+		if (__any_sync(FULL, found)) {
+			dist = s;
+			break;
+		}
+		if (n_e > c.w) ovf = true;
+		__syncwarp();
+
+		// ---- phase 2: in-vertex successors, sorted and unique by construction
+		// (gwf_ed_extend_batch, gwf-ed.cu:912-1016)
+		int32_t n_x = 0, n_tb = 0;
+		for (int32_t base = 0; base < n_a; base += 32) {
+			const int32_t j = base + lane;
+			uint64_t cv[3];
+			int32_t ck[3];
+			bool keep[3] = {false, false, false}, tmp[3] = {false, false, false};
+			if (j < n_a) {
+				const uint64_t vd = a_vd[j];
+				const int32_t k = a_k[j];
+				const int32_t vl = (int32_t)__ldg(g.len + vd_v(vd));
+				const uint64_t pv = j > 0 ? a_vd[j - 1] : 0;
+				const int32_t pk = j > 0 ? a_k[j - 1] : 0;
+				const uint64_t nv = j + 1 < n_a ? a_vd[j + 1] : 0;
+				const int32_t nk = j + 1 < n_a ? a_k[j + 1] : 0;
+				const bool left_in = j > 0 && pv == vd - 1, left2 = j > 0 && pv == vd - 2;
+				const bool right_in = j + 1 < n_a && nv == vd + 1, right2 = j + 1 < n_a && nv == vd + 2;
+				bool has[3];
+				// L: diagonal d-1 when absent from a: deletion from d, insertion from d-2
+				has[0] = !left_in;
+				cv[0] = vd - 1;
+				ck[0] = k + 1;
+				if (left2 && pk > ck[0]) ck[0] = pk;
+				// S: diagonal d: mismatch, insertion from d-1, deletion from d+1
+				has[1] = true;
+				cv[1] = vd;
+				ck[1] = k + 1;
+				if (left_in && pk > ck[1]) ck[1] = pk;
+				if (right_in && nk + 1 > ck[1]) ck[1] = nk + 1;
+				// R: diagonal d+1 when neither d+1 nor d+2 is in a: insertion from d
+				has[2] = !right_in && !right2;
+				cv[2] = vd + 1;
+				ck[2] = k;
+#pragma unroll
+				for (int t = 0; t < 3; ++t)
+					if (has[t]) {
+						const int32_t dd = vd_d(cv[t]);
+						if (dd + ck[t] < ql && ck[t] < vl) keep[t] = true;
+						else if (ck[t] == vl) tmp[t] = true;
+					}
+			}
+			int32_t tot, tott;
+			const int32_t nkeep = (int32_t)keep[0] + keep[1] + keep[2];
+			const int32_t ntmp = (int32_t)tmp[0] + tmp[1] + tmp[2];
+			int32_t off = warp_excl_scan(nkeep, &tot) + n_x;
+			int32_t offt = warp_excl_scan(ntmp, &tott) + n_tb;
+#pragma unroll
+			for (int t = 0; t < 3; ++t) {
+				if (keep[t]) {
+					if (off < c.x) x_vd[off] = cv[t], x_k[off] = ck[t];
+					++off;
+				}
+				if (tmp[t]) {
+					if (offt < c.tb) tb[offt] = cv[t];
+					++offt;
+				}
+			}
+			n_x += tot, n_tb += tott;
+		}
+		if (n_x > c.x || n_tb > c.tb) ovf = true;
+		__syncwarp();
+
+		// ---- phase 3: vertex-end states over arcs, in waves until no state is entered with a
+		// free match (gwf-ed.cu:1106-1255)
+		int32_t n_ba = 0, n_ta = 0;
+		for (int32_t wave = 0; n_e > 0 && !ovf; ++wave) {
+			if (wave > ql + 2) {
+				ovf = true;
+				break;
+			}
+			int32_t n_n = 0;
+			for (int32_t base = 0; base < n_e; base += 32) {
+				const int32_t j = base + lane;
+				bool act = j < n_e, isq = false, isv = false;
+				uint64_t vd = 0;
+				int32_t k = 0, d = 0, vl = 0, i = 0, nv = 0;
+				uint32_t v = 0, aoff = 0;
+				if (act) {
+					vd = e_vd[j], k = e_k[j];
+					v = vd_v(vd), d = vd_d(vd), vl = (int32_t)__ldg(g.len + v), i = d + k;
+					isq = i == ql - 1;
+					isv = !isq;
+					aoff = __ldg(g.arc_off + v);
+					const int32_t deg = (int32_t)(__ldg(g.arc_off + v + 1) - aoff);
+					if (isv || (k + 1 == vl && (int32_t)v != v1)) nv = deg;
+				}
+				// ended-diagonal point of a vertex-end state (gwf-ed.cu:1177-1183)
+				{
+					const uint32_t m = __ballot_sync(FULL, isv);
+					const int32_t pos = n_ta + __popc(m & lanemask_lt());
+					if (isv && pos < c.ta) ta[pos] = vd;
+					n_ta += __popc(m);
+				}
+				const int32_t max_nv = __reduce_max_sync(FULL, (uint32_t)nv);
+				int32_t n_ext = 0;
+				for (int32_t t = 0; t < max_nv; ++t) {
+					bool enter = false, two = false, one = false;
+					uint32_t w = 0;
+					int32_t ol = 0;
+					if (t < nv) {
+						const uint2 e = __ldg(g.arc + aoff + t);
+						w = e.x, ol = (int32_t)e.y;
+						if (isv) {
+							const int ins = hset_insert(h, hmask, (uint64_t)w << 32 | (uint32_t)(i + 1));
+							if (ins < 0) ovf = true;
+							const bool absent = ins == 1;
+							if (base_eq(g, rc, w, ol, i + 1)) {
+								++n_ext;
+								enter = absent;
+							} else
+								two = absent;
+							if (absent) ++n_keys; // per-lane; reduced below
+						} else
+							one = true; // v1 >= 0: query end at a vertex end, delete into w
+					}
+					const uint32_t me = __ballot_sync(FULL, enter);
+					const int32_t pe = n_n + __popc(me & lanemask_lt());
+					if (enter && pe < c.w) n_vd[pe] = gen_vd(w, i + 1 - ol), n_k[pe] = ol;
+					n_n += __popc(me);
+					int32_t tot;
+					int32_t pb = warp_excl_scan(two ? 2 : (one ? 1 : 0), &tot) + n_ba;
+					if (two) {
+						if (pb + 1 < c.ba) {
+							ba_vd[pb] = gen_vd(w, i - ol), ba_k[pb] = ol;         // deletion
+							ba_vd[pb + 1] = gen_vd(w, i + 1 - ol), ba_k[pb + 1] = ol; // mismatch
+						}
+					} else if (one) {
+						if (pb < c.ba) ba_vd[pb] = gen_vd(w, i - ol), ba_k[pb] = ol;
+					}
+					n_ba += tot;
+				}
+				// insertion at the vertex end (gwf-ed.cu:1225-1226); v1 >= 0 query-end deletion
+				// inside the vertex (gwf-ed.cu:1237-1241)
+				const bool ins = isv && (nv == 0 || n_ext != nv);
+				const bool qdel = isq && k + 1 < vl;
+				const uint32_t mi = __ballot_sync(FULL, ins || qdel);
+				const int32_t pi = n_ba + __popc(mi & lanemask_lt());
+				if ((ins || qdel) && pi < c.ba) {
+					ba_vd[pi] = ins ? gen_vd(v, d + 1) : gen_vd(v, d - 1);
+					ba_k[pi] = ins ? k : k + 1;
+				}
+				n_ba += __popc(mi);
+			}
+			{
+				int32_t tot;
+				warp_excl_scan(n_keys, &tot);
+				if (tot > hlimit) ovf = true;
+			}
+			if (n_n > c.w || n_ba > c.ba || n_ta > c.ta) ovf = true;
+			if (__any_sync(FULL, ovf)) {
+				ovf = true;
+				break;
+			}
+			__syncwarp();
+			// extend the entered states (gwf-ed.cu:1132-1160)
+			int32_t n_f = 0;
+			for (int32_t base = 0; base < n_n; base += 32) {
+				const int32_t j = base + lane;
+				bool toF = false, three = false;
+				uint64_t vd = 0;
+				int32_t k = 0, d = 0;
+				uint32_t v = 0;
+				if (j < n_n) {
+					vd = n_vd[j], k = n_k[j];
+					v = vd_v(vd), d = vd_d(vd);
+					const int32_t vl = (int32_t)__ldg(g.len + v);
+					k = ext(g, rc, v, d, k, vl);
+					const int32_t i = d + k;
+					if (i == ql - 1) {
+						if (v1 < 0 || ((int32_t)v == v1 && k == vl - 1)) found = true;
+						else toF = true;
+					} else if (k + 1 < vl)
+						three = true;
+					else
+						toF = true;
+				}
+				const uint32_t mf = __ballot_sync(FULL, toF);
+				const int32_t pf = n_f + __popc(mf & lanemask_lt());
+				if (toF && pf < c.w) f_vd[pf] = vd, f_k[pf] = k;
+				n_f += __popc(mf);
+				const uint32_t m3 = __ballot_sync(FULL, three);
+				const int32_t p3 = n_ba + 3 * __popc(m3 & lanemask_lt());
+				if (three && p3 + 2 < c.ba) {
+					ba_vd[p3] = gen_vd(v, d - 1), ba_k[p3] = k + 1;     // deletion
+					ba_vd[p3 + 1] = gen_vd(v, d), ba_k[p3 + 1] = k + 1; // mismatch
+					ba_vd[p3 + 2] = gen_vd(v, d + 1), ba_k[p3 + 2] = k; // insertion
+				}
+				n_ba += 3 * __popc(m3);
+			}
+			if (__any_sync(FULL, found)) break;
+			if (n_f > c.w || n_ba > c.ba) {
+				ovf = true;
+				break;
+			}
+			__syncwarp();
+			uint64_t *tv = e_vd;
+			int32_t *tk = e_k;
+			e_vd = f_vd, e_k = f_k, f_vd = tv, f_k = tk;
+			n_e = n_f;
+		}
+		if (__any_sync(FULL, found)) {
+			dist = s;
+			break;
+		}
+		if (__any_sync(FULL, ovf)) {
+			st = ST_CAPACITY;
+			break;
+		}
+		__syncwarp();
+
+		// ---- phase 4: ended-diagonal intervals, then the next wavefront
+		// (gwf_dedup / gwf_intv_merge2 / gwf_diag_dedup / gwf_mixed_dedup, gwf-ed.cu:780-804)
+		warp_bitonic_sort(ba_vd, ba_k, n_ba);
+		warp_bitonic_sort(ta, nullptr, n_ta);
+		// intervals: rank-merge the old ranges with both point lists, ties ordered I < TB < TA
+		const int32_t n_c = n_i + n_tb + n_ta;
+		if (n_c > c.iv + c.tb + c.ta) {
+			st = ST_CAPACITY;
+			break;
+		}
+		for (int32_t j = lane; j < n_i; j += 32) {
+			const uint64_t x = ilo[j];
+			const int32_t pos = j + lower_bound_u64(tb, n_tb, x) + lower_bound_u64(ta, n_ta, x);
+			clo[pos] = x, chi[pos] = ihi[j];
+		}
+		for (int32_t j = lane; j < n_tb; j += 32) {
+			const uint64_t x = tb[j];
+			const int32_t pos = j + upper_bound_u64(ilo, n_i, x) + lower_bound_u64(ta, n_ta, x);
+			clo[pos] = x, chi[pos] = x + 1;
+		}
+		for (int32_t j = lane; j < n_ta; j += 32) {
+			const uint64_t x = ta[j];
+			const int32_t pos = j + upper_bound_u64(ilo, n_i, x) + upper_bound_u64(tb, n_tb, x);
+			clo[pos] = x, chi[pos] = x + 1;
+		}
+		__syncwarp();
+		{ // coalesce overlapping or touching ranges (gwf_intv_merge_adj, gwf-ed.cu:266-296)
+			int32_t n_new = 0;
+			uint64_t carry = 0;
+			for (int32_t base = 0; base < n_c; base += 32) {
+				const int32_t j = base + lane;
+				const bool act = j < n_c;
+				const uint64_t lo = act ? clo[j] : 0, hi = act ? chi[j] : 0;
+				uint64_t pm = warp_incl_max(hi);
+				if (base > 0 && carry > pm) pm = carry;
+				uint64_t prev = __shfl_up_sync(FULL, pm, 1);
+				if (lane == 0) prev = carry;
+				const bool start = act && (j == 0 || lo > prev);
+				const bool end = act && (j + 1 == n_c || clo[j + 1] > pm);
+				const uint32_t ms = __ballot_sync(FULL, start);
+				if (start) {
+					const int32_t rk = n_new + __popc(ms & lanemask_lt());
+					if (rk < c.iv) ilo[rk] = lo;
+				}
+				if (end) {
+					const int32_t rk = n_new + __popc(ms & (lanemask_lt() | (1u << lane))) - 1;
+					if (rk < c.iv) ihi[rk] = pm;
+				}
+				n_new += __popc(ms);
+				carry = __shfl_sync(FULL, pm, 31);
+			}
+			n_i = n_new;
+		}
+		if (n_i > c.iv) {
+			st = ST_CAPACITY;
+			break;
+		}
+		__syncwarp();
+		// merge the in-vertex and arc-side candidates into a (ties: in-vertex first)
+		const int32_t n_m = n_x + n_ba;
+		for (int32_t j = lane; j < n_x; j += 32) {
+			const uint64_t x = x_vd[j];
+			const int32_t pos = j + lower_bound_u64(ba_vd, n_ba, x);
+			a_vd[pos] = x, a_k[pos] = x_k[j];
+		}
+		for (int32_t j = lane; j < n_ba; j += 32) {
+			const uint64_t x = ba_vd[j];
+			const int32_t pos = j + upper_bound_u64(x_vd, n_x, x);
+			a_vd[pos] = x, a_k[pos] = ba_k[j];
+		}
+		__syncwarp();
+		// keep the furthest k per diagonal, drop diagonals inside an ended interval
+		int32_t n_new = 0;
+		for (int32_t base = 0; base < n_m; base += 32) {
+			const int32_t j = base + lane;
+			bool keep = false;
+			uint64_t vd = 0;
+			int32_t k = 0;
+			if (j < n_m) {
+				vd = a_vd[j], k = a_k[j];
+				if (j == 0 || a_vd[j - 1] != vd) {
+					for (int32_t t = j + 1; t < n_m && a_vd[t] == vd; ++t) {
+						const int32_t kt = a_k[t];
+						k = kt > k ? kt : k;
+					}
+					keep = !in_ranges(ilo, ihi, n_i, vd);
+				}
+			}
+			__syncwarp();
+			const uint32_t m = __ballot_sync(FULL, keep);
+			if (keep) {
+				const int32_t pos = n_new + __popc(m & lanemask_lt());
+				a_vd[pos] = vd, a_k[pos] = k;
+			}
+			n_new += __popc(m);
+			__syncwarp();
+		}
+		n_a = n_new;
+		if (n_a == 0) break; // wavefront emptied: no alignment (gwf-ed.cu:1313, 1336)
+		if (n_a > c.a) {
+			st = ST_CAPACITY;
+			break;
+		}
+	}
+	if (lane == 0) {
+		p.dist[r] = st == ST_OK ? dist : -1;
+		p.status[r] = st;
+		if (st == ST_CAPACITY && p.retry_list) {
+			const int32_t q = atomicAdd(p.retry_n, 1);
+			p.retry_list[q] = r;
+		}
+		if (p.steps_out) p.steps_out[r] = steps;
+		if (p.w_out) p.w_out[r] = W;
+	}
+}
+
+// Plain form: one warp per queue position, arena offsets per read (main.cu:151-236 layout).
+__global__ void __launch_bounds__(256) k_align_plain(const KParams p)
+{
+	const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+	if (gw >= p.n_order) return;
+	const int32_t r = p.order[gw];
+	const Caps c = caps_for(p.r.ql[r], p.level, p.dens_milli);
+	align_read(p, r, p.ws + p.slot_off[gw], c);
+}
+
+// Persistent form: each warp owns one arena and pulls reads from the cost-ordered queue.
+__global__ void __launch_bounds__(256) k_align_persistent(const KParams p)
+{
+	const int lane = threadIdx.x & 31;
+	const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+	const Caps c = caps_for(p.ql_cap, p.level, p.dens_milli);
+	uint8_t *wsb = p.ws + gw * p.slot_bytes;
+	for (int32_t guard = 0; guard < p.n_order + 1; ++guard) {
+		int32_t qi = 0;
+		if (lane == 0) qi = atomicAdd(p.head, 1);
+		qi = __shfl_sync(FULL, qi, 0);
+		if (qi >= p.n_order) break;
+		align_read(p, p.order[qi], wsb, c);
+	}
+}
+
+// Packs reads to 2 bits per base (A=0 C=1 T=2 G=3 from bits 1-2 of the ASCII code) and flags
+// reads that contain anything but A/C/G/T. One warp per read; lane l builds words l, l+32, ...
+__global__ void __launch_bounds__(256) k_pack_reads(const uint8_t *__restrict__ raw,
+                                                    const int64_t *__restrict__ raw_off,
+                                                    const int32_t *__restrict__ ql,
+                                                    const int64_t *__restrict__ pk_off,
+                                                    uint64_t *__restrict__ pk, uint8_t *__restrict__ pure,
+                                                    int32_t n)
+{
+	const int lane = threadIdx.x & 31;
+	const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+	if (r >= n) return;
+	const uint8_t *q = raw + raw_off[r];
+	const int32_t L = ql[r] > 0 ? ql[r] : 0;
+	const int32_t nw = (L + 31) / 32 + 2;
+	uint64_t *out = pk + pk_off[r];
+	bool ok = true;
+	for (int32_t w = lane; w < nw; w += 32) {
+		uint64_t word = 0;
+		const int32_t b0 = w * 32;
+		for (int32_t t = 0; t < 32; ++t) {
+			const int32_t i = b0 + t;
+			if (i < L) {
+				const uint8_t ch = q[i];
+				ok &= (ch == 'A' || ch == 'C' || ch == 'G' || ch == 'T');
+				word |= (uint64_t)((ch >> 1) & 3) << (2 * t);
+			}
+		}
+		out[w] = word;
+	}
+	ok = __all_sync(FULL, ok);
+	if (lane == 0) pure[r] = ok ? 1 : 0;
+}
+
+} // namespace gwfb

@@ -1,0 +1,726 @@
+// gwf_runtime.cu — host side of libgwfa_b200: the C ABI declared in include/gwfa.h.
+//
+// gwf_ed_index builds the reference's host CSR (main.cu:246-270) and a device-resident copy of
+// the graph: vertex lengths, base offsets, 2-bit packed and raw sequences, CSR arcs. Batches run
+// on one stream: reads are copied once, packed on the device, aligned by the plain or the
+// persistent kernel, and reads whose arena overflowed are re-run at the next arena size class.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/gwfa.h"
+#include "gwf_kernels.cuh"
+#include "gwf_runtime.h"
+#include "gwfa_internal.h"
+
+using namespace gwfb;
+
+// ------------------------------------------------------------------ errors
+static thread_local char t_err[1024];
+
+void gwf_set_error(const char *msg) { snprintf(t_err, sizeof t_err, "%s", msg); }
+void gwf_set_errorf(const char *fmt, ...)
+{
+	va_list ap;
+	va_start(ap, fmt);
+	vsnprintf(t_err, sizeof t_err, fmt, ap);
+	va_end(ap);
+}
+extern "C" const char *gwf_last_error(void) { return t_err; }
+extern "C" const char *gwf_version(void) { return "gwfa-b200 0.1 (sm_100a)"; }
+
+#define CK(call)                                                                                    \
+	do {                                                                                            \
+		cudaError_t e_ = (call);                                                                    \
+		if (e_ != cudaSuccess) {                                                                    \
+			gwf_set_errorf("%s failed: %s", #call, cudaGetErrorString(e_));                        \
+			return GWF_E_CUDA;                                                                      \
+		}                                                                                           \
+	} while (0)
+
+// ------------------------------------------------------------------ buffers
+int DBuf::ensure(size_t n)
+{
+	if (n <= cap) return 0;
+	if (p) cudaFree(p);
+	p = nullptr, cap = 0;
+	size_t want = n + n / 4 + 256;
+	if (cudaMalloc(&p, want) != cudaSuccess) {
+		p = nullptr;
+		cudaGetLastError();
+		gwf_set_errorf("device allocation of %zu bytes failed", want);
+		return GWF_E_NOMEM;
+	}
+	cap = want;
+	return 0;
+}
+void DBuf::release()
+{
+	if (p) cudaFree(p);
+	p = nullptr, cap = 0;
+}
+
+int HBuf::ensure(size_t n)
+{
+	if (n <= cap) return 0;
+	if (p) cudaFreeHost(p);
+	p = nullptr, cap = 0;
+	size_t want = n + n / 4 + 256;
+	if (cudaMallocHost(&p, want) != cudaSuccess) {
+		p = nullptr;
+		cudaGetLastError();
+		gwf_set_errorf("pinned allocation of %zu bytes failed", want);
+		return GWF_E_NOMEM;
+	}
+	cap = want;
+	return 0;
+}
+void HBuf::release()
+{
+	if (p) cudaFreeHost(p);
+	p = nullptr, cap = 0;
+}
+
+// ------------------------------------------------------------------ device selection
+int gwf_select_device(int want, int *dev_out)
+{
+	int n = 0;
+	cudaError_t e = cudaGetDeviceCount(&n);
+	if (e != cudaSuccess || n == 0) {
+		cudaGetLastError();
+		gwf_set_errorf("no usable CUDA device: %s", e == cudaSuccess ? "none found" : cudaGetErrorString(e));
+		return GWF_E_CUDA;
+	}
+	int dev = want;
+	if (dev < 0) CK(cudaGetDevice(&dev));
+	if (dev >= n) {
+		gwf_set_error("device ordinal out of range");
+		return GWF_E_BAD_INPUT;
+	}
+	cudaDeviceProp prop;
+	CK(cudaGetDeviceProperties(&prop, dev));
+	if (prop.major != 10) {
+		gwf_set_errorf("device %d is sm_%d%d; this library is built for sm_100a (B200) only", dev,
+		               prop.major, prop.minor);
+		return GWF_E_CUDA;
+	}
+	CK(cudaSetDevice(dev));
+	*dev_out = dev;
+	return 0;
+}
+
+// ------------------------------------------------------------------ device graphs
+static std::mutex g_graph_mu;
+static std::unordered_map<const gwf_graph_t *, GraphDev *> g_graphs;
+
+DevGraph GraphDev::view() const
+{
+	DevGraph v;
+	v.len = (const uint32_t *)len.p;
+	v.base = (const uint64_t *)base.p;
+	v.pk = (const uint64_t *)pk.p;
+	v.raw = (const uint8_t *)raw.p;
+	v.arc_off = (const uint32_t *)arc_off.p;
+	v.arc = (const uint2 *)arc.p;
+	v.n_vtx = n_vtx;
+	v.pure = pure;
+	return v;
+}
+
+GraphDev::~GraphDev()
+{
+	int cur = -1;
+	cudaGetDevice(&cur);
+	if (device >= 0) cudaSetDevice(device);
+	len.release(), base.release(), pk.release(), raw.release(), arc_off.release(), arc.release();
+	if (cur >= 0) cudaSetDevice(cur);
+}
+
+GraphDev *gwf_find_graph(const gwf_graph_t *g)
+{
+	std::lock_guard<std::mutex> lk(g_graph_mu);
+	auto it = g_graphs.find(g);
+	return it == g_graphs.end() ? nullptr : it->second;
+}
+
+static uint8_t code2(uint8_t c) { return (uint8_t)((c >> 1) & 3); } // A0 C1 T2 G3
+
+static int upload_graph(const gwf_graph_t *g, GraphDev *G)
+{
+	const uint32_t nv = g->n_vtx;
+	std::vector<uint32_t> len(nv);
+	std::vector<uint64_t> base(nv);
+	uint64_t tot = 0;
+	for (uint32_t v = 0; v < nv; ++v) len[v] = g->len[v], base[v] = tot, tot += g->len[v];
+	const size_t nw = (size_t)((tot + 31) / 32 + 2);
+	std::vector<uint64_t> pk(nw, 0);
+	std::vector<uint8_t> raw((size_t)tot + 16, 0);
+	int pure = 1;
+	for (uint32_t v = 0; v < nv; ++v) {
+		const char *s = g->seq[v];
+		for (uint32_t j = 0; j < len[v]; ++j) {
+			const uint8_t c = (uint8_t)s[j];
+			const uint64_t p = base[v] + j;
+			raw[(size_t)p] = c;
+			if (c != 'A' && c != 'C' && c != 'G' && c != 'T') pure = 0;
+			pk[(size_t)(p >> 5)] |= (uint64_t)code2(c) << (2 * (p & 31));
+		}
+	}
+	std::vector<uint32_t> off(nv + 1, 0);
+	for (uint32_t e = 0; e < g->n_arc; ++e) off[(uint32_t)(g->arc[e].a >> 32) + 1]++;
+	for (uint32_t v = 0; v < nv; ++v) off[v + 1] += off[v];
+	std::vector<uint2> arc(g->n_arc ? g->n_arc : 1);
+	for (uint32_t e = 0; e < g->n_arc; ++e) arc[e] = make_uint2((uint32_t)g->arc[e].a, (uint32_t)g->arc[e].o);
+	G->n_vtx = nv, G->n_arc = g->n_arc, G->pure = pure, G->total_len = tot;
+	G->dens_milli = (int32_t)std::max<uint64_t>(1, (uint64_t)nv * 1000 / std::max<uint64_t>(1, tot));
+	int rc;
+	if ((rc = G->len.ensure(sizeof(uint32_t) * std::max<size_t>(nv, 1)))) return rc;
+	if ((rc = G->base.ensure(sizeof(uint64_t) * std::max<size_t>(nv, 1)))) return rc;
+	if ((rc = G->pk.ensure(sizeof(uint64_t) * nw))) return rc;
+	if ((rc = G->raw.ensure(raw.size()))) return rc;
+	if ((rc = G->arc_off.ensure(sizeof(uint32_t) * (nv + 1)))) return rc;
+	if ((rc = G->arc.ensure(sizeof(uint2) * arc.size()))) return rc;
+	CK(cudaMemcpy(G->len.p, len.data(), sizeof(uint32_t) * nv, cudaMemcpyHostToDevice));
+	CK(cudaMemcpy(G->base.p, base.data(), sizeof(uint64_t) * nv, cudaMemcpyHostToDevice));
+	CK(cudaMemcpy(G->pk.p, pk.data(), sizeof(uint64_t) * nw, cudaMemcpyHostToDevice));
+	CK(cudaMemcpy(G->raw.p, raw.data(), raw.size(), cudaMemcpyHostToDevice));
+	CK(cudaMemcpy(G->arc_off.p, off.data(), sizeof(uint32_t) * (nv + 1), cudaMemcpyHostToDevice));
+	CK(cudaMemcpy(G->arc.p, arc.data(), sizeof(uint2) * arc.size(), cudaMemcpyHostToDevice));
+	return 0;
+}
+
+extern "C" void gwf_ed_index(gwf_graph_t *g)
+{
+	if (!g) {
+		gwf_set_error("gwf_ed_index: null graph");
+		return;
+	}
+	// host CSR, as the reference (main.cu:246-270): arcs sorted by a, aux[v] = first << 32 | n
+	std::stable_sort(g->arc, g->arc + g->n_arc,
+	                 [](const gwf_arc_t &x, const gwf_arc_t &y) { return x.a < y.a; });
+	free(g->aux);
+	g->aux = (uint64_t *)calloc(g->n_vtx ? g->n_vtx : 1, sizeof(uint64_t));
+	for (uint32_t st = 0, i = 1; i <= g->n_arc; ++i)
+		if (i == g->n_arc || g->arc[i].a >> 32 != g->arc[st].a >> 32) {
+			const uint32_t v = (uint32_t)(g->arc[st].a >> 32);
+			if (v < g->n_vtx) g->aux[v] = (uint64_t)st << 32 | (i - st);
+			st = i;
+		}
+	// the device path needs well-formed input
+	for (uint32_t v = 0; v < g->n_vtx; ++v)
+		if (g->len[v] == 0 || !g->seq || !g->seq[v]) {
+			gwf_set_errorf("gwf_ed_index: vertex %u has no sequence", v);
+			return;
+		}
+	for (uint32_t e = 0; e < g->n_arc; ++e) {
+		const uint32_t s = (uint32_t)(g->arc[e].a >> 32), w = (uint32_t)g->arc[e].a;
+		if (s >= g->n_vtx || w >= g->n_vtx || g->arc[e].o < 0 || (uint32_t)g->arc[e].o >= g->len[w]) {
+			gwf_set_errorf("gwf_ed_index: arc %u (%u -> %u, overlap %d) is out of range", e, s, w,
+			               g->arc[e].o);
+			return;
+		}
+	}
+	int dev;
+	if (gwf_select_device(-1, &dev)) return; // host CSR stays usable; error recorded
+	GraphDev *G = new GraphDev;
+	G->device = dev;
+	if (upload_graph(g, G)) {
+		delete G;
+		return;
+	}
+	std::lock_guard<std::mutex> lk(g_graph_mu);
+	auto it = g_graphs.find(g);
+	if (it != g_graphs.end()) delete it->second;
+	g_graphs[g] = G;
+}
+
+extern "C" void gwf_cleanup(gwf_graph_t *g)
+{
+	if (!g) return;
+	free(g->aux);
+	g->aux = 0;
+	GraphDev *G = nullptr;
+	{
+		std::lock_guard<std::mutex> lk(g_graph_mu);
+		auto it = g_graphs.find(g);
+		if (it != g_graphs.end()) G = it->second, g_graphs.erase(it);
+	}
+	delete G;
+}
+
+// ------------------------------------------------------------------ engine
+Engine::~Engine()
+{
+	cudaSetDevice(device);
+	for (DBuf *b : {&pk_off, &order, &head, &retry_list, &retry_n, &ws, &slot_off, &w_out})
+		b->release();
+	for (HBuf *b : {&h_small}) b->release();
+	if (stream) cudaStreamDestroy(stream);
+	if (ev0) cudaEventDestroy(ev0);
+	if (ev1) cudaEventDestroy(ev1);
+}
+
+static std::mutex g_engine_mu;
+static std::unordered_map<int, Engine *> g_engines;
+
+Engine *gwf_engine(int dev)
+{
+	std::lock_guard<std::mutex> lk(g_engine_mu);
+	auto it = g_engines.find(dev);
+	if (it != g_engines.end()) return it->second;
+	Engine *E = new Engine;
+	E->device = dev;
+	cudaSetDevice(dev);
+	if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess ||
+	    cudaEventCreate(&E->ev0) != cudaSuccess || cudaEventCreate(&E->ev1) != cudaSuccess) {
+		cudaGetLastError();
+		gwf_set_error("stream/event creation failed");
+		delete E;
+		return nullptr;
+	}
+	cudaDeviceGetAttribute(&E->sm_count, cudaDevAttrMultiProcessorCount, dev);
+	int occ = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_align_persistent, 256, 0);
+	E->persistent_ctas_per_sm = occ > 0 ? occ : 1;
+	g_engines[dev] = E;
+	return E;
+}
+
+// ------------------------------------------------------------------ batches
+void Batch::release()
+{
+	for (DBuf *b : {&raw, &raw_off, &ql, &v0, &pk, &pk_off, &pure, &dist, &status, &steps, &order_ql})
+		b->release();
+}
+
+// Copies n reads (host, concatenated) into the batch's device buffers; computes host-side
+// layout (packed offsets, cost order).
+int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64_t *offs,
+                   const int32_t *ql, const int32_t *v0, int32_t v1)
+{
+	B.n = n, B.v1 = v1;
+	B.h_ql.assign(ql, ql + n);
+	int64_t lo = 0, hi = 0;
+	if (n > 0) {
+		lo = offs[0], hi = offs[0];
+		for (int32_t i = 0; i < n; ++i) {
+			if (ql[i] < 0) return GWF_E_BAD_INPUT;
+			lo = std::min(lo, offs[i]);
+			hi = std::max(hi, offs[i] + ql[i]);
+		}
+	}
+	B.h_raw_off.resize((size_t)n);
+	for (int32_t i = 0; i < n; ++i) B.h_raw_off[(size_t)i] = offs[i] - lo;
+	B.h_pk_off.resize((size_t)n);
+	int64_t words = 0;
+	for (int32_t i = 0; i < n; ++i) B.h_pk_off[(size_t)i] = words, words += (ql[i] + 31) / 32 + 2;
+	B.pk_words = words;
+	// persistent queue: longest reads first (LPT scheduling on a cost ~ length estimate)
+	B.h_order.resize((size_t)n);
+	std::iota(B.h_order.begin(), B.h_order.end(), 0);
+	std::stable_sort(B.h_order.begin(), B.h_order.end(),
+	                 [&](int32_t x, int32_t y) { return ql[x] > ql[y]; });
+	B.max_ql = 0;
+	for (int32_t i = 0; i < n; ++i) B.max_ql = std::max(B.max_ql, ql[i]);
+	const size_t nraw = (size_t)(hi - lo) + 16;
+	int rc;
+	if ((rc = B.raw.ensure(nraw)) || (rc = B.raw_off.ensure(8 * (size_t)n + 8)) ||
+	    (rc = B.ql.ensure(4 * (size_t)n + 4)) || (rc = B.v0.ensure(4 * (size_t)n + 4)) ||
+	    (rc = B.pk.ensure(8 * (size_t)words + 8)) || (rc = B.pk_off.ensure(8 * (size_t)n + 8)) ||
+	    (rc = B.pure.ensure((size_t)n + 8)) || (rc = B.dist.ensure(4 * (size_t)n + 4)) ||
+	    (rc = B.status.ensure(4 * (size_t)n + 4)) || (rc = B.steps.ensure(4 * (size_t)n + 4)) ||
+	    (rc = B.order_ql.ensure(4 * (size_t)n + 4)))
+		return rc;
+	cudaStream_t s = E.stream;
+	if (n > 0) {
+		CK(cudaMemcpyAsync(B.raw.p, seqs + lo, (size_t)(hi - lo), cudaMemcpyHostToDevice, s));
+		CK(cudaMemsetAsync((char *)B.raw.p + (hi - lo), 0, 16, s));
+		CK(cudaMemcpyAsync(B.raw_off.p, B.h_raw_off.data(), 8 * (size_t)n, cudaMemcpyHostToDevice, s));
+		CK(cudaMemcpyAsync(B.ql.p, ql, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+		CK(cudaMemcpyAsync(B.v0.p, v0, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+		CK(cudaMemcpyAsync(B.pk_off.p, B.h_pk_off.data(), 8 * (size_t)n, cudaMemcpyHostToDevice, s));
+		CK(cudaMemcpyAsync(B.order_ql.p, B.h_order.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+	}
+	return 0;
+}
+
+static DevReads reads_view(const Batch &B)
+{
+	DevReads r;
+	r.pk = (const uint64_t *)B.pk.p;
+	r.pk_off = (const int64_t *)B.pk_off.p;
+	r.raw = (const uint8_t *)B.raw.p;
+	r.raw_off = (const int64_t *)B.raw_off.p;
+	r.ql = (const int32_t *)B.ql.p;
+	r.v0 = (const int32_t *)B.v0.p;
+	r.pure = (const uint8_t *)B.pure.p;
+	r.v1 = B.v1;
+	r.n = B.n;
+	return r;
+}
+
+static KParams base_params(Engine &E, const GraphDev &G, Batch &B, int32_t flags)
+{
+	KParams p;
+	memset(&p, 0, sizeof p);
+	p.g = G.view();
+	p.r = reads_view(B);
+	p.dens_milli = G.dens_milli;
+	p.flags = flags;
+	p.dist = (int32_t *)B.dist.p;
+	p.status = (int32_t *)B.status.p;
+	p.retry_list = (int32_t *)E.retry_list.p;
+	p.retry_n = (int32_t *)E.retry_n.p;
+	p.steps_out = (int32_t *)B.steps.p;
+	p.w_out = nullptr;
+	return p;
+}
+
+static const int kWarpsPerCta = 8;
+static const int kMaxLevel = 3;
+
+// Persistent launch over the reads listed in d_order (device), arenas sized for ql_cap.
+static int launch_persistent(Engine &E, KParams p, const int32_t *d_order, int32_t n_order,
+                             int32_t ql_cap, int32_t level, int ctas_per_sm, int *launches)
+{
+	const Caps c = caps_for(ql_cap, level, p.dens_milli);
+	const int64_t slot = ws_layout(c).total;
+	int64_t warps = (int64_t)E.sm_count * ctas_per_sm * kWarpsPerCta;
+	const int64_t need_warps = (n_order + 0LL);
+	if (warps > need_warps) warps = std::max<int64_t>(kWarpsPerCta, ((need_warps + kWarpsPerCta - 1) / kWarpsPerCta) * kWarpsPerCta);
+	// keep arenas within a budget of the free device memory
+	size_t fr = 0, tot = 0;
+	cudaMemGetInfo(&fr, &tot);
+	const int64_t budget = (int64_t)(fr * 6 / 10) + (int64_t)E.ws.cap;
+	while (warps > kWarpsPerCta && warps * slot > budget) warps -= kWarpsPerCta;
+	if (warps * slot > budget) {
+		gwf_set_errorf("arena of %lld bytes per warp does not fit the device", (long long)slot);
+		return GWF_E_NOMEM;
+	}
+	int rc;
+	if ((rc = E.ws.ensure((size_t)(warps * slot)))) return rc;
+	if ((rc = E.head.ensure(16))) return rc;
+	CK(cudaMemsetAsync(E.head.p, 0, 4, E.stream));
+	p.order = d_order;
+	p.n_order = n_order;
+	p.head = (int32_t *)E.head.p;
+	p.ws = (uint8_t *)E.ws.p;
+	p.slot_bytes = slot;
+	p.level = level;
+	p.ql_cap = ql_cap;
+	const int ctas = (int)(warps / kWarpsPerCta);
+	k_align_persistent<<<ctas, 32 * kWarpsPerCta, 0, E.stream>>>(p);
+	CK(cudaGetLastError());
+	++*launches;
+	return 0;
+}
+
+// Plain launch: one warp per read in queue order, per-read arenas (split in chunks when the
+// arenas of all reads do not fit).
+static int launch_plain(Engine &E, KParams p, Batch &B, int *launches)
+{
+	size_t fr = 0, tot = 0;
+	cudaMemGetInfo(&fr, &tot);
+	const int64_t budget = (int64_t)(fr * 6 / 10) + (int64_t)E.ws.cap;
+	int32_t start = 0;
+	std::vector<int64_t> offs;
+	while (start < B.n) {
+		offs.clear();
+		int64_t used = 0;
+		int32_t end = start;
+		while (end < B.n) {
+			const int64_t sz = ws_layout(caps_for(B.h_ql[(size_t)end], 0, p.dens_milli)).total;
+			if (used + sz > budget && end > start) break;
+			offs.push_back(used);
+			used += sz;
+			++end;
+		}
+		int rc;
+		if ((rc = E.ws.ensure((size_t)used))) return rc;
+		if ((rc = E.slot_off.ensure(8 * offs.size()))) return rc;
+		if ((rc = E.order.ensure(4 * (size_t)(end - start)))) return rc;
+		std::vector<int32_t> ord((size_t)(end - start));
+		std::iota(ord.begin(), ord.end(), start);
+		CK(cudaMemcpyAsync(E.slot_off.p, offs.data(), 8 * offs.size(), cudaMemcpyHostToDevice, E.stream));
+		CK(cudaMemcpyAsync(E.order.p, ord.data(), 4 * ord.size(), cudaMemcpyHostToDevice, E.stream));
+		p.order = (const int32_t *)E.order.p;
+		p.n_order = end - start;
+		p.ws = (uint8_t *)E.ws.p;
+		p.slot_off = (const int64_t *)E.slot_off.p;
+		p.level = 0;
+		const int ctas = (p.n_order + kWarpsPerCta - 1) / kWarpsPerCta;
+		k_align_plain<<<ctas, 32 * kWarpsPerCta, 0, E.stream>>>(p);
+		CK(cudaGetLastError());
+		++*launches;
+		if (end < B.n) CK(cudaStreamSynchronize(E.stream)); // arenas are reused by the next chunk
+		start = end;
+	}
+	return 0;
+}
+
+int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t flags,
+                   int ctas_per_sm, float *ms, int *launches_out)
+{
+	int launches = 0, rc;
+	if (B.n == 0) {
+		if (ms) *ms = 0;
+		if (launches_out) *launches_out = 0;
+		return 0;
+	}
+	if ((rc = E.retry_list.ensure(4 * (size_t)B.n + 4)) || (rc = E.retry_n.ensure(16)) ||
+	    (rc = E.h_small.ensure(4 * (size_t)B.n + 64)))
+		return rc;
+	CK(cudaEventRecord(E.ev0, E.stream));
+	{
+		const int ctas = (B.n + kWarpsPerCta - 1) / kWarpsPerCta;
+		k_pack_reads<<<ctas, 32 * kWarpsPerCta, 0, E.stream>>>(
+		    (const uint8_t *)B.raw.p, (const int64_t *)B.raw_off.p, (const int32_t *)B.ql.p,
+		    (const int64_t *)B.pk_off.p, (uint64_t *)B.pk.p, (uint8_t *)B.pure.p, B.n);
+		CK(cudaGetLastError());
+		++launches;
+	}
+	CK(cudaMemsetAsync(E.retry_n.p, 0, 4, E.stream));
+	KParams p = base_params(E, G, B, flags);
+	if (ctas_per_sm <= 0) ctas_per_sm = E.persistent_ctas_per_sm;
+	if (mode == GWF_MODE_PLAIN) rc = launch_plain(E, p, B, &launches);
+	else rc = launch_persistent(E, p, (const int32_t *)B.order_ql.p, B.n, B.max_ql, 0, ctas_per_sm, &launches);
+	if (rc) return rc;
+	// re-run arena overflows at larger size classes
+	for (int level = 1; level <= kMaxLevel; ++level) {
+		int32_t nr = 0;
+		CK(cudaMemcpyAsync(E.h_small.p, E.retry_n.p, 4, cudaMemcpyDeviceToHost, E.stream));
+		CK(cudaStreamSynchronize(E.stream));
+		nr = *(int32_t *)E.h_small.p;
+		if (nr == 0) break;
+		std::vector<int32_t> ids((size_t)nr);
+		CK(cudaMemcpyAsync(E.h_small.p, E.retry_list.p, 4 * (size_t)nr, cudaMemcpyDeviceToHost, E.stream));
+		CK(cudaStreamSynchronize(E.stream));
+		memcpy(ids.data(), E.h_small.p, 4 * (size_t)nr);
+		int32_t cap = 0;
+		for (int32_t r : ids) cap = std::max(cap, B.h_ql[(size_t)r]);
+		std::sort(ids.begin(), ids.end(), [&](int32_t x, int32_t y) { return B.h_ql[(size_t)x] > B.h_ql[(size_t)y]; });
+		if ((rc = E.order.ensure(4 * (size_t)nr))) return rc;
+		CK(cudaMemcpyAsync(E.order.p, ids.data(), 4 * (size_t)nr, cudaMemcpyHostToDevice, E.stream));
+		CK(cudaMemsetAsync(E.retry_n.p, 0, 4, E.stream));
+		KParams q = p;
+		if (level == kMaxLevel) q.retry_list = nullptr; // last class: keep GWF_E_CAPACITY
+		if ((rc = launch_persistent(E, q, (const int32_t *)E.order.p, nr, cap, level, ctas_per_sm, &launches)))
+			return rc;
+	}
+	CK(cudaEventRecord(E.ev1, E.stream));
+	CK(cudaEventSynchronize(E.ev1));
+	if (ms) CK(cudaEventElapsedTime(ms, E.ev0, E.ev1));
+	if (launches_out) *launches_out = launches;
+	return 0;
+}
+
+int gwf_batch_fetch(Engine &E, Batch &B, int32_t *dist, int32_t *status)
+{
+	if (B.n == 0) return 0;
+	if (dist) CK(cudaMemcpyAsync(dist, B.dist.p, 4 * (size_t)B.n, cudaMemcpyDeviceToHost, E.stream));
+	if (status) CK(cudaMemcpyAsync(status, B.status.p, 4 * (size_t)B.n, cudaMemcpyDeviceToHost, E.stream));
+	CK(cudaStreamSynchronize(E.stream));
+	return 0;
+}
+
+// ------------------------------------------------------------------ public batch entry points
+static std::mutex g_batch_mu; // batch calls are serialised (one engine per device)
+static std::unordered_map<int, Batch *> g_scratch_batches;
+
+static int prepare(const gwf_graph_t *g, const gwf_batch_opts_t *opt, GraphDev **G, Engine **E)
+{
+	if (!g) {
+		gwf_set_error("null graph");
+		return GWF_E_BAD_INPUT;
+	}
+	*G = gwf_find_graph(g);
+	if (!*G) {
+		gwf_set_error("graph not indexed on a device: call gwf_ed_index first");
+		return GWF_E_NOT_INDEXED;
+	}
+	int dev;
+	int rc = gwf_select_device((*G)->device, &dev);
+	if (rc) return rc;
+	(void)opt;
+	*E = gwf_engine(dev);
+	return *E ? 0 : GWF_E_CUDA;
+}
+
+extern "C" int gwf_ed_batch_concat(const gwf_graph_t *g, int32_t n, const char *seqs,
+                                   const int64_t *offs, const int32_t *ql, const int32_t *v0,
+                                   int32_t v1, uint32_t max_lag, int32_t *dist, int32_t *status,
+                                   const gwf_batch_opts_t *opt)
+{
+	(void)max_lag; // accepted and ignored, as in the reference (gwf-ed.cu:1286-1287)
+	if (n < 0 || (n > 0 && (!seqs || !offs || !ql || !v0 || !dist))) {
+		gwf_set_error("bad batch arguments");
+		return GWF_E_BAD_INPUT;
+	}
+	GraphDev *G;
+	Engine *E;
+	int rc = prepare(g, opt, &G, &E);
+	if (rc) return rc;
+	if (v1 >= 0 && (uint32_t)v1 >= G->n_vtx) {
+		gwf_set_error("v1 out of range");
+		return GWF_E_BAD_INPUT;
+	}
+	std::lock_guard<std::mutex> lk(g_batch_mu);
+	Batch *&B = g_scratch_batches[E->device];
+	if (!B) B = new Batch;
+	if ((rc = gwf_batch_load(*E, *B, n, seqs, offs, ql, v0, v1))) return rc;
+	const int32_t mode = opt ? opt->mode : GWF_MODE_AUTO;
+	const int32_t flags = opt ? opt->flags : 0;
+	const int32_t cps = opt ? opt->ctas_per_sm : 0;
+	if ((rc = gwf_batch_exec(*E, *G, *B, mode, flags, cps, nullptr, nullptr))) return rc;
+	std::vector<int32_t> st;
+	if (!status) st.resize((size_t)n), status = st.data();
+	return gwf_batch_fetch(*E, *B, dist, status);
+}
+
+extern "C" int gwf_ed_batch(const gwf_graph_t *g, int32_t n, const char *const *q, const int32_t *ql,
+                            const int32_t *v0, int32_t v1, uint32_t max_lag, int32_t *dist,
+                            int32_t *status, const gwf_batch_opts_t *opt)
+{
+	if (n < 0 || (n > 0 && (!q || !ql || !v0 || !dist))) {
+		gwf_set_error("bad batch arguments");
+		return GWF_E_BAD_INPUT;
+	}
+	std::vector<int64_t> offs((size_t)n);
+	int64_t tot = 0;
+	for (int32_t i = 0; i < n; ++i) {
+		if (ql[i] < 0 || (ql[i] > 0 && !q[i])) {
+			gwf_set_error("bad read");
+			return GWF_E_BAD_INPUT;
+		}
+		offs[(size_t)i] = tot, tot += ql[i];
+	}
+	std::vector<char> cat((size_t)tot + 1);
+	for (int32_t i = 0; i < n; ++i) memcpy(cat.data() + offs[(size_t)i], q[i], (size_t)ql[i]);
+	return gwf_ed_batch_concat(g, n, cat.data(), offs.data(), ql, v0, v1, max_lag, dist, status, opt);
+}
+
+extern "C" int32_t gwf_ed(void *km, const gwf_graph_t *g, int32_t ql, const char *q, int32_t v0,
+                          int32_t v1, uint32_t max_lag, int32_t traceback)
+{
+	(void)km; // kalloc.c is empty in the reference
+	if (traceback != 0) {
+		gwf_set_error("traceback is not implemented by the reference path");
+		return GWF_E_UNSUPPORTED;
+	}
+	if (!g || !q || ql <= 0) {
+		gwf_set_error("gwf_ed: empty or null query");
+		return GWF_E_BAD_INPUT;
+	}
+	if (v0 < 0 || (uint32_t)v0 >= g->n_vtx || (v1 >= 0 && (uint32_t)v1 >= g->n_vtx)) {
+		gwf_set_error("gwf_ed: v0/v1 out of range");
+		return GWF_E_BAD_INPUT;
+	}
+	int64_t off = 0;
+	int32_t dist = -1, status = 0;
+	gwf_batch_opts_t opt;
+	memset(&opt, 0, sizeof opt);
+	opt.mode = GWF_MODE_PERSISTENT;
+	int rc = gwf_ed_batch_concat(g, 1, q, &off, &ql, &v0, v1, max_lag, &dist, &status, &opt);
+	if (rc) return rc;
+	if (status != GWF_OK) return status;
+	return dist;
+}
+
+// ------------------------------------------------------------------ resident batches
+struct gwf_batch_s {
+	const gwf_graph_t *g;
+	Batch B;
+	int launches = 0;
+};
+
+extern "C" gwf_batch_t *gwf_batch_create(const gwf_graph_t *g, int32_t n, const char *seqs,
+                                         const int64_t *offs, const int32_t *ql, const int32_t *v0,
+                                         int32_t v1, const gwf_batch_opts_t *opt)
+{
+	GraphDev *G;
+	Engine *E;
+	if (prepare(g, opt, &G, &E)) return nullptr;
+	if (n < 0 || (n > 0 && (!seqs || !offs || !ql || !v0))) {
+		gwf_set_error("bad batch arguments");
+		return nullptr;
+	}
+	gwf_batch_s *b = new gwf_batch_s;
+	b->g = g;
+	std::lock_guard<std::mutex> lk(g_batch_mu);
+	if (gwf_batch_load(*E, b->B, n, seqs, offs, ql, v0, v1) || cudaStreamSynchronize(E->stream) != cudaSuccess) {
+		b->B.release();
+		delete b;
+		return nullptr;
+	}
+	return b;
+}
+
+extern "C" int gwf_batch_run(gwf_batch_t *b, const gwf_batch_opts_t *opt, float *kernel_ms)
+{
+	if (!b) return GWF_E_BAD_INPUT;
+	GraphDev *G;
+	Engine *E;
+	int rc = prepare(b->g, opt, &G, &E);
+	if (rc) return rc;
+	std::lock_guard<std::mutex> lk(g_batch_mu);
+	return gwf_batch_exec(*E, *G, b->B, opt ? opt->mode : GWF_MODE_AUTO, opt ? opt->flags : 0,
+	                      opt ? opt->ctas_per_sm : 0, kernel_ms, &b->launches);
+}
+
+extern "C" int gwf_batch_results(gwf_batch_t *b, int32_t *dist, int32_t *status)
+{
+	if (!b) return GWF_E_BAD_INPUT;
+	GraphDev *G;
+	Engine *E;
+	int rc = prepare(b->g, nullptr, &G, &E);
+	if (rc) return rc;
+	std::lock_guard<std::mutex> lk(g_batch_mu);
+	return gwf_batch_fetch(*E, b->B, dist, status);
+}
+
+extern "C" int32_t gwf_batch_launches(const gwf_batch_t *b) { return b ? b->launches : 0; }
+
+extern "C" int gwf_batch_steps(gwf_batch_t *b, int32_t *steps)
+{
+	if (!b || !steps) return GWF_E_BAD_INPUT;
+	GraphDev *G;
+	Engine *E;
+	int rc = prepare(b->g, nullptr, &G, &E);
+	if (rc) return rc;
+	std::lock_guard<std::mutex> lk(g_batch_mu);
+	if (b->B.n == 0) return 0;
+	CK(cudaMemcpyAsync(steps, b->B.steps.p, 4 * (size_t)b->B.n, cudaMemcpyDeviceToHost, E->stream));
+	CK(cudaStreamSynchronize(E->stream));
+	return 0;
+}
+
+extern "C" void gwf_batch_destroy(gwf_batch_t *b)
+{
+	if (!b) return;
+	b->B.release();
+	delete b;
+}
+
+extern "C" void *gwf_pinned_alloc(int64_t bytes)
+{
+	void *p = nullptr;
+	if (bytes <= 0 || cudaMallocHost(&p, (size_t)bytes) != cudaSuccess) {
+		cudaGetLastError();
+		gwf_set_error("pinned allocation failed");
+		return nullptr;
+	}
+	return p;
+}
+
+extern "C" void gwf_pinned_free(void *p)
+{
+	if (p) cudaFreeHost(p);
+}

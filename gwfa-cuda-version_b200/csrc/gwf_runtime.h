@@ -1,0 +1,62 @@
+// gwf_runtime.h — internal host structures of libgwfa_b200 (device graphs, engines, batches).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/gwfa.h"
+#include "gwf_device.cuh"
+
+struct DBuf { // grow-only device buffer
+	void *p = nullptr;
+	size_t cap = 0;
+	int ensure(size_t n);
+	void release();
+};
+
+struct HBuf { // grow-only pinned host buffer
+	void *p = nullptr;
+	size_t cap = 0;
+	int ensure(size_t n);
+	void release();
+};
+
+struct GraphDev { // device-resident copy of one gwf_graph_t
+	int device = -1;
+	uint32_t n_vtx = 0, n_arc = 0;
+	int32_t pure = 0, dens_milli = 1;
+	uint64_t total_len = 0;
+	DBuf len, base, pk, raw, arc_off, arc;
+	gwfb::DevGraph view() const;
+	~GraphDev();
+};
+
+struct Engine { // per-device launch state: stream, events, warp arenas
+	int device = 0;
+	int sm_count = 0;
+	int persistent_ctas_per_sm = 1;
+	cudaStream_t stream = nullptr;
+	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+	DBuf pk_off, order, head, retry_list, retry_n, ws, slot_off, w_out;
+	HBuf h_small;
+	~Engine();
+};
+
+struct Batch { // reads resident on the device
+	int32_t n = 0, v1 = -1, max_ql = 0;
+	int64_t pk_words = 0;
+	std::vector<int32_t> h_ql, h_order;
+	std::vector<int64_t> h_raw_off, h_pk_off;
+	DBuf raw, raw_off, ql, v0, pk, pk_off, pure, dist, status, steps, order_ql;
+	void release();
+};
+
+GraphDev *gwf_find_graph(const gwf_graph_t *g);
+Engine *gwf_engine(int dev);
+int gwf_select_device(int want, int *dev_out);
+int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64_t *offs,
+                   const int32_t *ql, const int32_t *v0, int32_t v1);
+int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t flags,
+                   int ctas_per_sm, float *ms, int *launches_out);
+int gwf_batch_fetch(Engine &E, Batch &B, int32_t *dist, int32_t *status);

@@ -1,0 +1,166 @@
+/*
+ * gwfa.h — drop-in C ABI of the B200 GWFA sequence-to-graph edit-distance path.
+ *
+ * The graph types keep the exact layout of the reference's gwfa.h:6-18, so a caller that
+ * already builds a gwf_graph_t (for example through gwf_gfa2gwf, main.cu:294-345) passes it
+ * unchanged. Every entry point is plain C: pointers and sizes, no CUDA or C++ types.
+ *
+ * Error model: functions returning int return 0 on success or a negative GWF_E_* code.
+ * gwf_ed returns the distance (>= 0), -1 when no alignment exists (reference behaviour,
+ * gwf-ed.cu:1336), or a GWF_E_* code (<= -2). gwf_last_error() gives a message for the
+ * last failure in the calling thread.
+ */
+#ifndef GWFA_B200_H
+#define GWFA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- graph types: same layout as the reference (gwfa.h:6-18) ---- */
+typedef struct {
+	uint64_t a; /* source vertex << 32 | target vertex */
+	int32_t o;  /* overlap on the target: the walk enters the target at offset o */
+} gwf_arc_t;
+
+typedef struct {
+	uint32_t n_vtx, n_arc;
+	uint32_t *len;   /* vertex lengths */
+	uint32_t *src;   /* original oriented GFA vertex (segment << 1 | strand) */
+	char **seq;      /* NUL-terminated vertex sequences */
+	gwf_arc_t *arc;  /* arcs; sorted by a after gwf_ed_index */
+	uint64_t *aux;   /* CSR: first_arc << 32 | n_arcs per vertex, filled by gwf_ed_index */
+} gwf_graph_t;
+
+/* ---- status / error codes ---- */
+#define GWF_OK               0
+#define GWF_NO_ALIGNMENT    (-1) /* distance value: wavefront emptied (gwf-ed.cu:1336) */
+#define GWF_E_BAD_INPUT     (-2) /* ql <= 0, v0/v1 out of range, null pointer */
+#define GWF_E_UNSUPPORTED   (-3) /* traceback != 0 or max_lag != 0: the reference has neither */
+#define GWF_E_CAPACITY      (-4) /* read did not fit the largest wavefront arena class */
+#define GWF_E_CUDA          (-5) /* CUDA runtime failure or no usable B200 device */
+#define GWF_E_NOT_INDEXED   (-6) /* gwf_ed_index was not called for this graph */
+#define GWF_E_BAD_GRAPH     (-7) /* zero-length vertex, arc overlap >= target length, bad CSR */
+#define GWF_E_TIMEOUT       (-8) /* a bounded device/host wait gave up (serving loop) */
+#define GWF_E_NOMEM         (-9) /* device or host allocation failed */
+#define GWF_E_BUSY          (-10) /* serving admission refused: arena budget exhausted */
+
+/* batch flags */
+#define GWF_F_EXACT_START   0x1 /* extend the start state even when v0 or the query is shorter
+                                   than 32 bases. The reference skips that extension
+                                   (gwf-ed.cu:809,833: k=-1 compared against an unsigned
+                                   max_k), which adds cost for reads whose origin vertex is short.
+                                   Default off = reference-identical distances. */
+
+/* execution forms */
+#define GWF_MODE_AUTO        0 /* persistent cost-ordered queue */
+#define GWF_MODE_PLAIN       1 /* one launch per batch, one warp per read */
+#define GWF_MODE_PERSISTENT  2 /* persistent kernel fed by a cost-ordered device queue */
+
+typedef struct {
+	int32_t mode;        /* GWF_MODE_* */
+	int32_t flags;       /* GWF_F_* */
+	int32_t device;      /* CUDA device ordinal (-1 = current) */
+	int32_t warps_per_cta; /* 0 = autotuned */
+	int32_t ctas_per_sm;   /* 0 = autotuned (persistent form) */
+	int32_t use_graph;     /* 1 = capture the launch sequence in a CUDA graph (persistent) */
+	int32_t reserved[10];
+} gwf_batch_opts_t;
+
+/* ---- index / cleanup (reference gwfa.h:87-88, main.cu:246-277) ---- */
+
+/* Replaces gwf_ed_index (main.cu:265-270): sorts g->arc by a, fills g->aux (calloc'd, as the
+ * reference does) and uploads a device-resident CSR with 2-bit packed vertex sequences to the
+ * current CUDA device. The device copy is kept in a side table keyed by g. On a device failure
+ * the host CSR is still built; gwf_last_error() reports the device error. */
+void gwf_ed_index(gwf_graph_t *g);
+
+/* Replaces gwf_cleanup (main.cu:273-277): frees g->aux and the device copy of g. */
+void gwf_cleanup(gwf_graph_t *g);
+
+/* Host-callable single alignment. Replaces the device-only
+ * gwf_ed(g, ql, q, v0, v1, max_lag, buf, diag_shared) of gwfa.h:95 with the upstream GWFA
+ * signature. km is accepted and ignored (kalloc.c is empty in the reference). Synchronous.
+ * Returns the edit distance, -1 if no alignment, or a GWF_E_* code. */
+int32_t gwf_ed(void *km, const gwf_graph_t *g, int32_t ql, const char *q, int32_t v0, int32_t v1,
+               uint32_t max_lag, int32_t traceback);
+
+/* Batch alignment of n reads given as separate strings. Replaces the caller-side stream loop of
+ * main.cu:620-735 plus gwf_ed_kernel (main.cu:151-236). v0 is per read (the reference kernel
+ * hard-codes 0, main.cu:217). dist[i] receives the distance or -1; status[i] GWF_OK or a
+ * per-read GWF_E_* code. Returns 0, or a negative code when the whole call failed. */
+int gwf_ed_batch(const gwf_graph_t *g, int32_t n, const char *const *q, const int32_t *ql,
+                 const int32_t *v0, int32_t v1, uint32_t max_lag, int32_t *dist, int32_t *status,
+                 const gwf_batch_opts_t *opt);
+
+/* Same as gwf_ed_batch with the reads concatenated in one host buffer (the layout of
+ * all_sequences_host in main.cu:481-531): read i is seqs[offs[i] .. offs[i]+ql[i]). */
+int gwf_ed_batch_concat(const gwf_graph_t *g, int32_t n, const char *seqs, const int64_t *offs,
+                        const int32_t *ql, const int32_t *v0, int32_t v1, uint32_t max_lag,
+                        int32_t *dist, int32_t *status, const gwf_batch_opts_t *opt);
+
+/* ---- device-resident batches (inputs uploaded once; used to time the kernel alone) ---- */
+typedef struct gwf_batch_s gwf_batch_t;
+gwf_batch_t *gwf_batch_create(const gwf_graph_t *g, int32_t n, const char *seqs,
+                              const int64_t *offs, const int32_t *ql, const int32_t *v0,
+                              int32_t v1, const gwf_batch_opts_t *opt);
+/* Runs the whole batch on the device (including overflow retries). Returns 0 or GWF_E_*.
+ * *kernel_ms receives the device time of the run measured with CUDA events. */
+int gwf_batch_run(gwf_batch_t *b, const gwf_batch_opts_t *opt, float *kernel_ms);
+int gwf_batch_results(gwf_batch_t *b, int32_t *dist, int32_t *status);
+/* Number of kernel launches issued by the last gwf_batch_run. */
+int32_t gwf_batch_launches(const gwf_batch_t *b);
+/* Score steps each read took in the last run (diagnostics and cost models). */
+int gwf_batch_steps(gwf_batch_t *b, int32_t *steps);
+void gwf_batch_destroy(gwf_batch_t *b);
+
+/* Page-locked host memory for read buffers, so that batch copies run at full PCIe speed. */
+void *gwf_pinned_alloc(int64_t bytes);
+void gwf_pinned_free(void *p);
+
+/* ---- serving: continuous batching on a resident graph ---- */
+typedef struct gwf_srv_s gwf_srv_t;
+typedef struct {
+	int64_t arena_budget_bytes; /* device bytes for in-flight wavefront arenas */
+	int32_t max_inflight_reads; /* slots of the running kernel; 0 = derived from the budget */
+	int32_t flags;              /* GWF_F_* */
+	int32_t device;
+	int32_t reserved[7];
+} gwf_srv_opts_t;
+gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t *opt);
+/* Queues one request of n reads; returns a request id >= 0 or a GWF_E_* code. Copies the
+ * reads, so the caller's buffers can be reused on return. */
+int64_t gwf_srv_submit(gwf_srv_t *s, int32_t n, const char *seqs, const int64_t *offs,
+                       const int32_t *ql, const int32_t *v0, int32_t v1);
+/* 1 = done (dist/status filled), 0 = pending, < 0 = error. */
+int gwf_srv_poll(gwf_srv_t *s, int64_t req, int32_t *dist, int32_t *status);
+/* Waits at most timeout_s seconds. Returns 1 done, GWF_E_TIMEOUT, or another error. */
+int gwf_srv_wait(gwf_srv_t *s, int64_t req, int32_t *dist, int32_t *status, double timeout_s);
+/* Completion and admission timestamps (seconds, steady clock) of a finished request. */
+int gwf_srv_times(gwf_srv_t *s, int64_t req, double *t_submit, double *t_admit, double *t_done);
+void gwf_srv_destroy(gwf_srv_t *s);
+
+/* ---- GFA input side (reference gfa-io.c, gfa-base.c, gfa-sub.c, main.cu:294-359) ---- */
+
+/* gfa_read + gfa_finalize + gwf_gfa2gwf in one call. start_seg = segment name of v0, forward
+ * strand (main.cu:399-407); NULL = first segment. Returns NULL on failure. */
+gwf_graph_t *gwf_gfa_load(const char *path, const char *start_seg);
+/* Same from an in-memory GFA text. */
+gwf_graph_t *gwf_gfa_load_mem(const char *text, int64_t len, const char *start_seg);
+/* Frees a graph from gwf_gfa_load* (gwf_free, main.cu:347-352); also calls gwf_cleanup. */
+void gwf_graph_free(gwf_graph_t *g);
+/* Writes the gwf_graph_print dump (main.cu:354-359) to buf. Returns the full length; writes at
+ * most cap bytes (NUL-terminated when it fits). */
+int64_t gwf_graph_dump(const gwf_graph_t *g, char *buf, int64_t cap);
+
+/* ---- diagnostics ---- */
+const char *gwf_last_error(void);
+const char *gwf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
