@@ -1,0 +1,345 @@
+"""Benchmark of the GWFA sequence-to-graph edit-distance path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload config2] [--impl ours|reference]
+
+One step = one pass of the path over the whole workload (default: 100,000 reads of 1 kbp, 50,000
+at 5% and 50,000 at 10% error, on the 100 kbp bubble graph; synthetic and seeded). `value` is
+reads/s with the reads already resident in HBM (CUDA events on the library's stream, L2 flushed
+between steps); `e2e` is the same metric through gwf_ed_batch_concat from pinned host memory,
+with the copies in the timed region. Under torchrun every rank aligns its own workload (weak
+scaling, no data-path collective); timings are the max over ranks.
+`--impl reference` times the reference algorithm on the host cores instead (the reference ships
+no CPU gwf_ed; its CPU restatement in oracle/ stands in for it).
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "reads/sec and Gbases/sec (bit-exact), persistent-batched vs plain kernel; serving p50/p99"
+WORKLOAD_DESC = {
+    "config1": "config1: 1,000 reads x 1 kbp at 1% on the 100 kbp bubble graph",
+    "config2": "config2: 100,000 reads x 1 kbp (50,000 at 5%, 50,000 at 10%) on the 100 kbp bubble graph",
+    "config3": "config3: 200,000 reads, lognormal length (median 2 kbp, sigma 0.6, 500-10000 bp), error U[1%,10%]",
+    "config4": "config4: 20,000 reads x 10 kbp at 5% on the 5 Mbp graph (variant every 50 bp, SV every 50 kbp)",
+}
+
+
+def pkg():
+    import importlib.util
+    d = os.path.join(ROOT, "gwfa-cuda-version_b200")
+    if "gwfa_b200" in sys.modules:
+        return sys.modules["gwfa_b200"]
+    spec = importlib.util.spec_from_file_location("gwfa_b200", os.path.join(d, "__init__.py"),
+                                                  submodule_search_locations=[d])
+    m = importlib.util.module_from_spec(spec)
+    sys.modules["gwfa_b200"] = m
+    spec.loader.exec_module(m)
+    return m
+
+
+def oracle_mod():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    return oracle
+
+
+def shard_seed(workload, rank):
+    """Per-rank seed: rank 0 uses the published workload seeds, others shift them."""
+    return None if rank == 0 else 1000 + 17 * rank
+
+
+class ClockSampler:
+    """nvidia-smi clocks during the timed region (one sample every 200 ms)."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(lens, W, E):
+    """Bytes per read: ql + 4 + 32 W + 2 E (query, result, one 16-byte state read and written
+    per wavefront diagonal per step, one graph and one query byte per compared character)."""
+    return float(np.sum(lens.astype(np.float64) + 4 + 32.0 * W + 2.0 * E))
+
+
+def cpu_oracle_run(w, max_seconds=30.0, threads=0):
+    """Oracle over the workload with all host threads. Runs the whole workload when a probe
+    predicts it finishes within max_seconds, else a prefix sample of each error class."""
+    O = oracle_mod()
+    og = O.OracleGraph.from_graph(w["graph"])
+    n = len(w["lens"])
+    probe = min(n, 2000)
+    idx_probe = np.linspace(0, n - 1, probe).astype(np.int64)
+    t0 = time.perf_counter()
+    _, _, used = og.ed_batch(w["cat"], w["offs"][idx_probe], w["lens"][idx_probe], w["v0"][idx_probe],
+                             stats=False, threads=threads)
+    tp = time.perf_counter() - t0
+    est = tp * n / probe
+    if est <= max_seconds:
+        sel = np.arange(n)
+    else:
+        m = max(probe, int(n * max_seconds / est))
+        sel = np.linspace(0, n - 1, m).astype(np.int64)
+    t0 = time.perf_counter()
+    dist, st, used = og.ed_batch(w["cat"], w["offs"][sel], w["lens"][sel], w["v0"][sel], stats=True,
+                                 threads=threads)
+    el = time.perf_counter() - t0
+    s = O.stats_arrays(st, len(sel))
+    return {"sel": sel, "dist": dist, "W": s["W"], "E": s["E"], "flags": s["flags"], "seconds": el,
+            "threads": used, "full": len(sel) == n}
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference algorithm on the host cores (oracle port, all threads)."""
+    if rank != 0:
+        return
+    G = pkg()
+    w = G.load_workload(args.workload)
+    O = oracle_mod()
+    og = O.OracleGraph.from_graph(w["graph"])
+    n = len(w["lens"])
+    # each step aligns a bounded, evenly spread sample so the whole run takes a few minutes
+    budget_s = args.ref_step_seconds
+    probe = np.linspace(0, n - 1, min(n, 1000)).astype(np.int64)
+    t0 = time.perf_counter()
+    _, _, threads = og.ed_batch(w["cat"], w["offs"][probe], w["lens"][probe], w["v0"][probe], stats=False)
+    per_read = (time.perf_counter() - t0) / len(probe)
+    m = int(min(n, max(len(probe), budget_s / max(per_read, 1e-9))))
+    sel = np.linspace(0, n - 1, m).astype(np.int64)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        og.ed_batch(w["cat"], w["offs"][sel], w["lens"][sel], w["v0"][sel], stats=False)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    ms = 1000.0 * statistics.mean(times)
+    rps = m / (ms / 1000.0)
+    bases = float(np.sum(w["lens"][sel]))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rps, "unit": "reads/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC[args.workload], "sample_reads_per_step": m},
+        "gbases_per_s": bases / (ms / 1000.0) / 1e9,
+        "cpu_baseline": {"value": rps, "unit": "reads/s", "cores": threads, "kind": "port",
+                         "sample": "%d of %d reads per step, evenly spread" % (m, n)},
+        "e2e": {"value": rps, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="config2", choices=sorted(WORKLOAD_DESC))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="persistent", choices=["persistent", "plain"])
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--ref-step-seconds", type=float, default=8.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    G = pkg()
+    mode = G.MODE_PERSISTENT if args.mode == "persistent" else G.MODE_PLAIN
+    w = G.load_workload(args.workload, seed=shard_seed(args.workload, rank), pinned=True)
+    g = w["graph"]
+    g.index()
+    n = len(w["lens"])
+    bases = float(np.sum(w["lens"]))
+    batch = G.ResidentBatch(g, w["cat"], w["offs"], w["lens"], w["v0"], mode=mode)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        batch.run(mode=mode)
+    dist_gpu, status = batch.results()
+    launches = 0
+    times = []
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()              # evict L2 between steps (256 MB > 126 MB L2)
+            torch.cuda.synchronize()
+            times.append(batch.run(mode=mode))
+            launches += batch.launches()
+        torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(statistics.mean(times))
+    value = world * n / (ms / 1000.0)
+
+    # the other form on the same reads, for the persistent-vs-plain comparison
+    forms = {}
+    if not args.no_plain:
+        other = G.MODE_PLAIN if mode == G.MODE_PERSISTENT else G.MODE_PERSISTENT
+        batch.run(mode=other)
+        t2 = []
+        for _ in range(max(1, min(args.steps, 3))):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t2.append(batch.run(mode=other))
+        d2, _ = batch.results()
+        ms2 = max_over_ranks(statistics.mean(t2))
+        forms = {args.mode: n / (ms / 1000.0),
+                 ("plain" if other == G.MODE_PLAIN else "persistent"): n / (ms2 / 1000.0),
+                 "forms_identical": bool(np.array_equal(d2, dist_gpu))}
+
+    # end to end through the public batch call, pinned host buffers, copies in the timed region
+    out_d = np.zeros(n, np.int32)
+    out_s = np.zeros(n, np.int32)
+    for _ in range(2):
+        g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode)
+    e2e_t = []
+    barrier()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        out_d, out_s = g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode)
+        e2e_t.append(time.perf_counter() - t0)
+    barrier()
+    e2e_s = max_over_ranks(statistics.mean(e2e_t))
+    h2d = int(w["offs"][-1] + w["lens"][-1]) + n * (8 + 4 + 4 + 8 + 4)
+    d2h = n * 8 + 4
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC[args.workload], "reads_per_gpu": n, "form": args.mode,
+                   "l2": "flushed between steps (256 MB write)", "parallelism": "reads sharded by rank, graph replicated"},
+        "gbases_per_s": world * bases / (ms / 1000.0) / 1e9,
+        "e2e": {"value": world * n / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "status_ok": bool((status == 0).all()),
+        "clocks": clk.summary(),
+    }
+    if forms:
+        line["forms"] = forms
+
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_oracle_run(w)
+        sel = cpu["sel"]
+        line["bit_exact_vs_oracle"] = {"reads_checked": int(len(sel)),
+                                       "mismatches": int(np.sum(cpu["dist"] != dist_gpu[sel]))}
+        line["cpu_baseline"] = {"value": len(sel) / cpu["seconds"], "unit": "reads/s", "cores": cpu["threads"],
+                                "kind": "port",
+                                "sample": ("whole workload" if cpu["full"] else "%d evenly spread reads" % len(sel))
+                                + ", oracle/gwf_oracle.c restatement of gwf-ed.cu, all host threads"}
+        scale = n / len(sel)
+        alg = algorithmic_bytes(w["lens"][sel], cpu["W"], cpu["E"]) * scale
+        peak, src = measured_peak()
+        achieved = alg / (ms / 1000.0) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic_%s.json" % args.workload)
+        if os.path.exists(tp):
+            traffic = json.load(open(tp)).get("dram_bytes_per_launch")
+        line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "traffic": traffic,
+                            "peak_source": src + " hbm_gbs (burst)",
+                            "algorithmic_bytes_per_step": alg,
+                            "note": "B_read = ql + 4 + 32 W + 2 E per read, W/E from the oracle"
+                                    + ("" if cpu["full"] else " sample, scaled")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

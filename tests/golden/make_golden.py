@@ -1,0 +1,149 @@
+"""Generates the golden fixtures of tests/golden/ from the reference itself.
+
+Stages (run in order):
+  prepare   (CPU, needs the reference tree): copies the reference's exposed fixtures
+            (graph_1000.gfa, grafo_test.gfa, the first 200 reads of reads_1000.fa) into
+            tests/golden/, records the reference loader's `gwf-test -p` dumps, and writes the
+            synthetic read sets to _work/golden_inputs/ as FASTA + per-read v0. Reads that the
+            oracle flags as unsafe for the reference (arena overflow, non-termination) are
+            left out, so the reference kernel is never given an input that can fault or hang.
+  run       (GPU box): runs oracle/_ref/gwf-test and oracle/_ref/gwf-ref-harness (the
+            reference's own CUDA code, built by `make -C oracle ref`) on those inputs; writes
+            gpurun_out/golden/*.txt.
+  collect   (CPU): copies the reference outputs into tests/golden/ref_*.txt.
+
+    python tests/golden/make_golden.py prepare
+    python tests/golden/make_golden.py run        # under gpurun
+    python tests/golden/make_golden.py collect
+"""
+import importlib.util
+import json
+import os
+import shutil
+import subprocess
+import sys
+
+import numpy as np
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
+GOLD = os.path.join(ROOT, "tests", "golden")
+INP = os.path.join(ROOT, "_work", "golden_inputs")
+OUT = os.path.join(ROOT, "gpurun_out", "golden")
+REF = "/root/reference"
+
+# synthetic sets: name -> (workload, n reads)
+SYNTH = {"config1": ("config1", 1000), "config2": ("config2", 2000), "config3": ("config3", 600)}
+
+
+def pkg():
+    spec = importlib.util.spec_from_file_location(
+        "gwfa_b200", os.path.join(ROOT, "gwfa-cuda-version_b200", "__init__.py"),
+        submodule_search_locations=[os.path.join(ROOT, "gwfa-cuda-version_b200")])
+    m = importlib.util.module_from_spec(spec)
+    sys.modules["gwfa_b200"] = m
+    spec.loader.exec_module(m)
+    return m
+
+
+def oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as o
+    return o
+
+
+def read_fasta(path, limit=None):
+    reads = []
+    for line in open(path, "rb"):
+        line = line.rstrip(b"\r\n")
+        if line.startswith(b">"):
+            if limit is not None and len(reads) >= limit:
+                break
+            reads.append(b"")
+        elif reads:
+            reads[-1] += line
+    return reads
+
+
+def write_fasta(path, reads):
+    with open(path, "wb") as f:
+        for i, r in enumerate(reads):
+            f.write(b">r%d\n%s\n" % (i, r))
+
+
+def prepare():
+    G, O = pkg(), oracle()
+    os.makedirs(INP, exist_ok=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all", "ref"], check=True)
+    gwf_test = os.path.join(ROOT, "oracle", "_ref", "gwf-test")
+    shutil.copy(os.path.join(REF, "exposed_testing/1000_reads/graph_1000.gfa"), GOLD)
+    shutil.copy(os.path.join(REF, "exposed_testing/generated/grafo_test.gfa"), GOLD)
+    reads = read_fasta(os.path.join(REF, "exposed_testing/1000_reads/reads_1000.fa"), limit=200)
+    write_fasta(os.path.join(GOLD, "reads_200.fa"), reads)
+    for name in ("graph_1000", "grafo_test"):
+        dump = subprocess.run([gwf_test, "-p", os.path.join(GOLD, name + ".gfa")], capture_output=True).stdout
+        open(os.path.join(GOLD, name + ".ref_dump.txt"), "wb").write(dump)
+    # exposed reads: all start at the first segment (gwf-test's default v0)
+    g = G.Graph.from_gfa(os.path.join(GOLD, "graph_1000.gfa"))
+    og = O.OracleGraph.from_graph(g)
+    cat, offs, lens = G.pack_reads(reads)
+    d, st, _ = og.ed_batch(cat, offs, lens, 0)
+    flags = O.stats_arrays(st, len(lens))["flags"]
+    assert not (flags & O.F_UNSAFE_MASK).any(), "exposed reads unsafe for the reference"
+    # synthetic sets
+    manifest = {}
+    for name, (kind, n) in SYNTH.items():
+        w = G.load_workload(kind, n=n)
+        og = O.OracleGraph.from_graph(w["graph"])
+        d, st, _ = og.ed_batch(w["cat"], w["offs"], w["lens"], w["v0"])
+        flags = O.stats_arrays(st, n)["flags"]
+        keep = np.nonzero((flags & O.F_UNSAFE_MASK) == 0)[0]
+        open(os.path.join(INP, name + ".gfa"), "wb").write(w["synth"].gfa)
+        rr = [w["cat"][w["offs"][i]:w["offs"][i] + w["lens"][i]].tobytes() for i in keep]
+        write_fasta(os.path.join(INP, name + ".fa"), rr)
+        np.savetxt(os.path.join(INP, name + ".v0.txt"), w["v0"][keep], fmt="%d")
+        manifest[name] = {"workload": kind, "n": n, "kept": keep.tolist()}
+    json.dump(manifest, open(os.path.join(INP, "manifest.json"), "w"))
+    print("prepared", {k: len(v["kept"]) for k, v in manifest.items()})
+
+
+def run():
+    os.makedirs(OUT, exist_ok=True)
+    R = os.path.join(ROOT, "oracle", "_ref")
+    res = subprocess.run([os.path.join(R, "gwf-test"), os.path.join(GOLD, "graph_1000.gfa"),
+                          os.path.join(GOLD, "reads_200.fa")], capture_output=True, text=True, timeout=600)
+    if res.returncode != 0:
+        raise SystemExit("gwf-test failed: " + res.stderr[-2000:])
+    open(os.path.join(OUT, "exposed_gwf_test.txt"), "w").write(res.stdout)
+    for name in SYNTH:
+        res = subprocess.run([os.path.join(R, "gwf-ref-harness"), os.path.join(INP, name + ".gfa"),
+                              os.path.join(INP, name + ".fa"), os.path.join(INP, name + ".v0.txt")],
+                             capture_output=True, text=True, timeout=900)
+        if res.returncode != 0:
+            raise SystemExit(name + " harness failed: " + res.stderr[-2000:])
+        open(os.path.join(OUT, name + ".txt"), "w").write(res.stdout)
+        open(os.path.join(OUT, name + ".timing.json"), "w").write(res.stderr.strip().splitlines()[-1])
+    print("ran reference on", ["exposed"] + list(SYNTH))
+
+
+def collect():
+    # gwf-test prints a header, one distance per read, then a timing line (main.cu:470, 747-750)
+    lines = open(os.path.join(OUT, "exposed_gwf_test.txt")).read().split("\n")
+    vals = [int(x) for x in lines if x.strip().lstrip("-").isdigit()]
+    with open(os.path.join(GOLD, "ref_exposed_200.txt"), "w") as f:
+        f.write("# reference gwf-test (sm_100a build of the reference sources) on graph_1000.gfa + reads_200.fa\n")
+        f.write("\n".join(str(v) for v in vals) + "\n")
+    man = json.load(open(os.path.join(INP, "manifest.json")))
+    for name in SYNTH:
+        vals = [int(x) for x in open(os.path.join(OUT, name + ".txt")).read().split()]
+        kept = man[name]["kept"]
+        assert len(vals) == len(kept)
+        with open(os.path.join(GOLD, "ref_%s.txt" % name), "w") as f:
+            f.write("# reference gwf_ed (gwf-ed.cu via oracle/_ref/gwf-ref-harness) on load_workload(%r, n=%d);"
+                    " columns: read index, distance\n" % (man[name]["workload"], man[name]["n"]))
+            for i, v in zip(kept, vals):
+                f.write("%d %d\n" % (i, v))
+    print("collected")
+
+
+if __name__ == "__main__":
+    {"prepare": prepare, "run": run, "collect": collect}[sys.argv[1]]()

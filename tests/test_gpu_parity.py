@@ -1,0 +1,130 @@
+"""GPU parity: every int32 distance from the sm_100a kernels equals the oracle (CPU restatement
+of gwf-ed.cu) and the reference's own CUDA outputs, bit for bit. All calls go through the C ABI
+of libgwfa_b200.so."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLD, read_fasta, read_golden
+from randgraph import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _indexed(G, g):
+    err = g.index()
+    assert g.indexed
+    return g
+
+
+def test_exposed_reads_match_reference(G, O):
+    _, ref = read_golden("ref_exposed_200.txt")
+    reads = read_fasta(os.path.join(GOLD, "reads_200.fa"))
+    g = _indexed(G, G.Graph.from_gfa(os.path.join(GOLD, "graph_1000.gfa")))
+    for mode in (G.MODE_PLAIN, G.MODE_PERSISTENT):
+        d, st = g.ed_batch(reads, 0, mode=mode)
+        assert (st == 0).all()
+        assert list(d) == ref
+
+
+@pytest.mark.parametrize("name,n", [("config1", 1000), ("config2", 2000), ("config3", 600)])
+def test_synthetic_match_reference_and_oracle(G, O, name, n):
+    idx, ref = read_golden("ref_%s.txt" % name)
+    w = G.load_workload(name, n=n)
+    g = _indexed(G, w["graph"])
+    sel = np.array(idx)
+    for mode in (G.MODE_PLAIN, G.MODE_PERSISTENT):
+        d, st = g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode)
+        assert (st == 0).all()
+        assert list(d[sel]) == ref
+        og = O.OracleGraph.from_graph(w["graph"])
+        od, _, _ = og.ed_batch(w["cat"], w["offs"], w["lens"], w["v0"], stats=False)
+        assert np.array_equal(d, od)
+
+
+@pytest.mark.parametrize("exact", [False, True])
+def test_random_graphs_match_oracle(G, O, exact):
+    """Small DAGs and cyclic graphs, 1-base vertices (start-state quirk), N and lower-case
+    bytes (byte-compare path), v1 >= 0 targets."""
+    flags = G.GWF_F_EXACT_START if exact else 0
+    checked = 0
+    for t, (seqs, arcs, v0, v1, q) in enumerate(cases(303 + exact, 250, v1_prob=0.25)):
+        g = _indexed(G, G.Graph.from_arrays(seqs, arcs))
+        og = O.OracleGraph(seqs, arcs)
+        od, ost = og.ed(q, v0, v1, exact_start=exact)
+        if ost.flags & O.F_NONTERM:
+            continue
+        d, st = g.ed_batch([q], [v0], v1=v1, flags=flags, mode=G.MODE_PLAIN if t % 2 else G.MODE_PERSISTENT)
+        assert st[0] == 0 and d[0] == od, (seqs, arcs, v0, v1, q, d[0], od)
+        if exact and v1 < 0:
+            assert d[0] == og.dp(q, v0, v1)
+        checked += 1
+        g.close()
+    assert checked > 200
+
+
+def test_single_read_entry_point(G, O):
+    w = G.load_workload("config1", n=20)
+    g = _indexed(G, w["graph"])
+    og = O.OracleGraph.from_graph(w["graph"])
+    for i in range(20):
+        q = w["cat"][w["offs"][i]:w["offs"][i] + w["lens"][i]].tobytes()
+        assert g.ed(q, int(w["v0"][i])) == og.ed(q, int(w["v0"][i]))[0]
+    # max_lag is accepted and ignored, as in the reference; traceback is not implemented
+    q = w["cat"][:w["lens"][0]].tobytes()
+    assert g.ed(q, int(w["v0"][0]), max_lag=7) == og.ed(q, int(w["v0"][0]))[0]
+    with pytest.raises(G.GwfError):
+        g.ed(q, int(w["v0"][0]), traceback=1)
+
+
+def test_pointer_array_batch_equals_concat(G):
+    w = G.load_workload("config1", n=64)
+    g = _indexed(G, w["graph"])
+    a, _ = g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], concat=True)
+    b, _ = g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], concat=False)
+    assert np.array_equal(a, b)
+
+
+def test_edge_cases(G, O):
+    seqs, arcs = [b"ACGTACGT", b"TTTT"], [(0, 1, 0)]
+    g = _indexed(G, G.Graph.from_arrays(seqs, arcs))
+    og = O.OracleGraph(seqs, arcs)
+    d, st = g.ed_batch([b"", b"ACGT", b"N", b"ACGTACGTTTTTGGGG"], [0, 5, 0, 0])
+    assert st[0] == G.GWF_E_BAD_INPUT and st[1] == G.GWF_E_BAD_INPUT
+    assert st[2] == 0 and st[3] == 0
+    # the 8-base start vertex does not extend at score 0 (reference start-state rule): +1
+    assert d[3] == og.ed(b"ACGTACGTTTTTGGGG", 0)[0] == og.dp(b"ACGTACGTTTTTGGGG", 0) + 1 == 5
+    d, st = g.ed_batch([b"ACGTACGTTTTTGGGG"], [0], flags=G.GWF_F_EXACT_START)
+    assert d[0] == 4
+    d, st = g.ed_batch([], [], mode=G.MODE_PERSISTENT)
+    assert len(d) == 0
+    # a read that can only be aligned with insertions past the graph end
+    q = b"ACGTACGTTTTT" + b"C" * 30
+    d, st = g.ed_batch([q], [0], flags=G.GWF_F_EXACT_START)
+    assert st[0] == 0 and d[0] == 30 == og.dp(q, 0)
+
+
+def test_long_reads_dense_graph_and_retries(G, O):
+    """10 kbp reads on the 5 Mbp dense graph (config 4 shapes): large wavefronts, arrival sets
+    of ~10^5 keys; reads whose arena overflows are re-run at a larger class."""
+    w = G.load_workload("config4", n=24)
+    g = _indexed(G, w["graph"])
+    d, st = g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"])
+    assert (st == 0).all()
+    og = O.OracleGraph.from_graph(w["graph"])
+    od, _, _ = og.ed_batch(w["cat"], w["offs"], w["lens"], w["v0"], stats=False)
+    assert np.array_equal(d, od)
+
+
+def test_resident_batch_runs_are_repeatable(G):
+    w = G.load_workload("config1", n=500)
+    g = _indexed(G, w["graph"])
+    b = G.ResidentBatch(g, w["cat"], w["offs"], w["lens"], w["v0"])
+    ms = b.run()
+    d1, _ = b.results()
+    b.run(mode=G.MODE_PLAIN)
+    d2, _ = b.results()
+    assert ms > 0 and np.array_equal(d1, d2)
+    assert b.launches() >= 2
+    assert (b.steps() == d1 + 1).all()
