@@ -207,7 +207,7 @@ struct ReadCtx {
 	const uint8_t *qraw;  // raw query bytes
 	int32_t ql, v1;
 	bool packed;          // graph and read are A/C/G/T only
-	bool quirk;           // reference start-state behaviour (see ext)
+	bool quirk;           // reference start-state rules (ext, and the k=-1 filter of step 2)
 };
 
 // gwf_extend1 (gwf-ed.cu:806-839): last matching offset on diagonal d from offset k. With

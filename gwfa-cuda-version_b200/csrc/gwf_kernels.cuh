@@ -158,11 +158,14 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				has[2] = !right_in && !right2;
 				cv[2] = vd + 1;
 				ck[2] = k;
+				// the reference keeps vl in a uint32_t here (gwf-ed.cu:895, 993): a candidate
+				// with k = -1 (insertion before the first base of v0) fails `k < vl` and is dropped
 #pragma unroll
 				for (int t = 0; t < 3; ++t)
 					if (has[t]) {
 						const int32_t dd = vd_d(cv[t]);
-						if (dd + ck[t] < ql && ck[t] < vl) keep[t] = true;
+						const bool kin = rc.quirk ? (uint32_t)ck[t] < (uint32_t)vl : ck[t] < vl;
+						if (dd + ck[t] < ql && kin) keep[t] = true;
 						else if (ck[t] == vl) tmp[t] = true;
 					}
 			}

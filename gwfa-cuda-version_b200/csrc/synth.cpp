@@ -80,7 +80,7 @@ Graph *make_graph(int64_t L, int32_t every, double p_snp, int32_t indel_max, int
 	struct Ev { int64_t pos; int type; int64_t len; }; // 0 SNP, 1 INS, 2 DEL
 	std::vector<Ev> ev;
 	int64_t sv_next = sv_every > 0 ? sv_every : -1, sv_block_end = -1;
-	int64_t margin = (int64_t)(indel_max > sv_max ? indel_max : sv_max) + 2;
+	int64_t margin = (int64_t)(sv_every > 0 && sv_max > indel_max ? sv_max : indel_max) + 2;
 	for (int64_t p = every; p + margin < L; p += every) {
 		if (sv_next > 0 && p >= sv_next) {
 			int64_t len = sv_min + (int64_t)rng.below((uint32_t)(sv_max - sv_min + 1));

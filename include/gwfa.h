@@ -48,11 +48,14 @@ typedef struct {
 #define GWF_E_BUSY          (-10) /* serving admission refused: arena budget exhausted */
 
 /* batch flags */
-#define GWF_F_EXACT_START   0x1 /* extend the start state even when v0 or the query is shorter
-                                   than 32 bases. The reference skips that extension
-                                   (gwf-ed.cu:809,833: k=-1 compared against an unsigned
-                                   max_k), which adds cost for reads whose origin vertex is short.
-                                   Default off = reference-identical distances. */
+#define GWF_F_EXACT_START   0x1 /* exact edit distance at the start of the read. By default the
+                                   library reproduces two reference rules about the start state
+                                   k = -1: gwf_extend1 does not extend it when v0 or the query is
+                                   shorter than 32 bases (signed k against an unsigned max_k,
+                                   gwf-ed.cu:809,833), and gwf_ed_extend_batch drops insertion
+                                   candidates with k = -1 (uint32_t vl, gwf-ed.cu:895,993), so an
+                                   alignment cannot begin with an insertion. Both add cost to
+                                   some reads. Default off = reference-identical distances. */
 
 /* execution forms */
 #define GWF_MODE_AUTO        0 /* persistent cost-ordered queue */

@@ -6,13 +6,16 @@
  * warp-parallel step of the reference (ballot compactions, merge-path merges, parallel sorts)
  * becomes the serial loop it computes. Each function cites the reference lines it restates.
  *
- * It reproduces the reference's observable behaviour, including three quirks found by reading:
+ * It reproduces the reference's observable behaviour, including four quirks found by reading:
  *  1. gwf_extend1 (gwf-ed.cu:806-839) compares a signed k against an unsigned max_k. With
  *     k = -1 the serial tail loop never runs, so the start state does not extend when
  *     min(ql - d, vl) < 32. GWFO_O_EXACT_START disables this for the ground-truth comparison.
  *  2. gwf_diag_is_sorted / gwf_intv_is_sorted (gwf-ed.cu:219-263, 372-417) skip element 32 and,
  *     when n <= 33, the last element. ref_is_sorted() emulates the 32 lanes literally.
- *  3. The reference never terminates when the first query-end state it pops has k = -1
+ *  3. gwf_ed_extend_batch (gwf-ed.cu:895, 993) holds the vertex length in a uint32_t, so its
+ *     successor filter `p->k < vl` drops every candidate with k = -1: an alignment cannot begin
+ *     with an insertion before the first base of v0. GWFO_O_EXACT_START disables this too.
+ *  4. The reference never terminates when the first query-end state it pops has k = -1
  *     (gwf-ed.cu:1233 sets end_off = -1, gwf-ed.cu:1327 then keeps looping). The oracle stops,
  *     returns s and sets GWFO_F_NONTERM.
  * Capacity limits of the reference arena (main.cu:498-505) are emulated where they are safe
@@ -429,10 +432,13 @@ static void o_extend_batch(ows_t *w, int32_t n, int32_t off)
 			A_push(w, vd[j], ak[j], xo[j]);
 		}
 	}
+	/* vl is uint32_t in the reference (gwf-ed.cu:895), so `p->k < vl` is an unsigned compare:
+	 * a candidate with k = -1 (an insertion before the first base of the vertex) is dropped */
 	for (j = 0, m = 0; j < n + 2; ++j) {
 		od_t *p = &b[j];
 		int32_t d = (int32_t)p->vd - SHIFT;
-		if (d + p->k < ql && p->k < vl) b[m++] = *p;
+		int k_ok = (w->opts & GWFO_O_EXACT_START) ? p->k < vl : (uint32_t)p->k < (uint32_t)vl;
+		if (d + p->k < ql && k_ok) b[m++] = *p;
 		else if (p->k == vl) tmp_push(w, gen_vd(v, d));
 	}
 	w->n_B += m;

@@ -29,7 +29,8 @@ extern "C" {
 #define GWFO_F_UNSAFE_MASK  0x7f0
 
 /* options */
-#define GWFO_O_EXACT_START  0x1 /* disable the k=-1 unsigned-compare quirk (see gwf_oracle.c) */
+#define GWFO_O_EXACT_START  0x1 /* disable the two k=-1 unsigned-compare rules of the start
+                                     state (see gwf_oracle.c): exact edit distance */
 
 typedef struct {
 	int32_t steps;        /* score steps executed (s + 1 when an end is found) */
