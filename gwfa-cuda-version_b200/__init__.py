@@ -80,6 +80,7 @@ SIGNATURES = {
     "gwf_batch_launches": (I32, [P]),
     "gwf_batch_steps": (ctypes.c_int, [P, P]),
     "gwf_batch_destroy": (None, [P]),
+    "gwf_ed_batch_noalloc": (ctypes.c_int, [PG, I32, I32, P, P, P, P, I32, P, P, I32, P]),
     "gwf_pinned_alloc": (P, [I64]),
     "gwf_pinned_free": (None, [P]),
     "gwf_srv_create": (P, [PG, P]),

@@ -26,6 +26,7 @@ struct KParams {
 	int64_t *w_out;         // optional per-read sum of wavefront sizes
 };
 
+#ifndef GWF_KERNELS_DECL_ONLY
 // Aligns read r with one warp. All control flow is warp-uniform.
 __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *wsb, const Caps &c)
 {
@@ -513,5 +514,6 @@ __global__ void __launch_bounds__(256) k_pack_reads(const uint8_t *__restrict__ 
 	ok = __all_sync(FULL, ok);
 	if (lane == 0) pure[r] = ok ? 1 : 0;
 }
+#endif // GWF_KERNELS_DECL_ONLY
 
 } // namespace gwfb

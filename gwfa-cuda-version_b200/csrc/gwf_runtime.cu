@@ -531,6 +531,13 @@ int gwf_batch_fetch(Engine &E, Batch &B, int32_t *dist, int32_t *status)
 	return 0;
 }
 
+// Launches the persistent kernel with parameters built by the caller (gwf_ed_batch_noalloc).
+cudaError_t gwf_launch_persistent(const KParams &p, int ctas, int threads, cudaStream_t s)
+{
+	k_align_persistent<<<ctas, threads, 0, s>>>(p);
+	return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ public batch entry points
 static std::mutex g_batch_mu; // batch calls are serialised (one engine per device)
 static std::unordered_map<int, Batch *> g_scratch_batches;

@@ -60,3 +60,7 @@ int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64
 int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t flags,
                    int ctas_per_sm, float *ms, int *launches_out);
 int gwf_batch_fetch(Engine &E, Batch &B, int32_t *dist, int32_t *status);
+namespace gwfb {
+struct KParams;
+}
+cudaError_t gwf_launch_persistent(const gwfb::KParams &p, int ctas, int threads, cudaStream_t s);

@@ -119,6 +119,30 @@ int32_t gwf_batch_launches(const gwf_batch_t *b);
 int gwf_batch_steps(gwf_batch_t *b, int32_t *steps);
 void gwf_batch_destroy(gwf_batch_t *b);
 
+/* ---- batch alignment that allocates nothing ----
+ * No counterpart in the reference. For callers that must not allocate device memory while they
+ * align, such as a framework whose caching allocator owns the device heap, or a latency-bound
+ * serving loop that cannot afford cudaMalloc's implicit device synchronisation. The caller passes
+ * device buffers; the call allocates nothing. Its warp arenas live in one fixed device array of
+ * GWF_NOALLOC_SCRATCH_BYTES (64 MiB) that every GPU loading the library holds until exit.
+ * Limits: at most GWF_NOALLOC_MAX_READS reads per call and GWF_NOALLOC_MAX_QL bases per read
+ * (max_ql = the longest read; larger calls return GWF_E_CAPACITY), and a read whose wavefront
+ * outgrows its arena gets per-read status GWF_E_CAPACITY (there is no larger arena to retry in).
+ * Layout: read i is d_seqs[d_offs[i] .. d_offs[i]+d_ql[i]); d_seqs must be 8-byte aligned with
+ * 16 readable bytes after the last read. The graph must have been indexed on the current device
+ * (gwf_ed_index). Asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream):
+ * d_dist / d_status are valid once the stream has completed. The first call on a device does a
+ * one-time set-up (symbol lookup and a small init kernel); make that first call before any
+ * stream capture. All calls share the one array, so calls that overlap on the GPU (e.g. on two
+ * streams) race; serialise them. Returns 0 or a GWF_E_* code. */
+#define GWF_NOALLOC_MAX_READS     262144
+#define GWF_NOALLOC_MAX_QL        2048
+#define GWF_NOALLOC_SCRATCH_BYTES (64LL << 20)
+int gwf_ed_batch_noalloc(const gwf_graph_t *g, int32_t n, int32_t max_ql, const char *d_seqs,
+                         const int64_t *d_offs, const int32_t *d_ql, const int32_t *d_v0,
+                         int32_t v1, int32_t *d_dist, int32_t *d_status, int32_t flags,
+                         void *stream);
+
 /* Page-locked host memory for read buffers, so that batch copies run at full PCIe speed. */
 void *gwf_pinned_alloc(int64_t bytes);
 void gwf_pinned_free(void *p);
