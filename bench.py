@@ -202,6 +202,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-step-seconds", type=float, default=8.0)
+    ap.add_argument("--ctas-per-sm", type=int, default=0, help="persistent grid; 0 = occupancy limit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -246,7 +247,7 @@ def main():
         return float(t.item())
 
     for _ in range(args.warmup):
-        batch.run(mode=mode)
+        batch.run(mode=mode, ctas_per_sm=args.ctas_per_sm)
     dist_gpu, status = batch.results()
     launches = 0
     times = []
@@ -256,7 +257,7 @@ def main():
         for _ in range(args.steps):
             flush.zero_()              # evict L2 between steps (256 MB > 126 MB L2)
             torch.cuda.synchronize()
-            times.append(batch.run(mode=mode))
+            times.append(batch.run(mode=mode, ctas_per_sm=args.ctas_per_sm))
             launches += batch.launches()
         torch.cuda.synchronize()
     barrier()

@@ -34,6 +34,7 @@ constexpr int32_t ST_BAD_INPUT = -2;
 constexpr int32_t ST_CAPACITY = -4;
 
 struct DevGraph {
+	const uint4 *vtx;        // [n_vtx] (base low 32 bits, base high 32 bits, length, first arc)
 	const uint32_t *len;     // [n_vtx]
 	const uint64_t *base;    // [n_vtx] first base of the vertex in the concatenated sequence
 	const uint64_t *pk;      // 2-bit packed sequence, 32 bases per word, +2 padding words
@@ -54,6 +55,14 @@ struct DevReads {
 	const uint8_t *pure;    // 1 when the read is A/C/G/T only
 	int32_t v1;
 	int32_t n;
+};
+
+// One wavefront state: diagonal vd and offset k of the last matched base (16 bytes, one vector
+// load or store).
+struct __align__(16) St {
+	uint64_t vd;
+	int32_t k;
+	int32_t pad;
 };
 
 // Per-warp arena capacities (entries).
@@ -107,9 +116,10 @@ __host__ __device__ inline Caps caps_for(int32_t ql, int32_t level, int32_t dens
 }
 
 struct WsOff { // byte offsets in one warp arena
-	int64_t a_vd, a_k, x_vd, x_k, ba_vd, ba_k, w0_vd, w0_k, w1_vd, w1_k, n_vd, n_k, tb, ta, i0_lo,
-	    i0_hi, i1_lo, i1_hi, h, total;
+	int64_t h, a, x, ba, w0, w1, nw, tb, ta, i0_lo, i0_hi, i1_lo, i1_hi, total;
 };
+// The wavefront ping-pongs between the a and x buffers (x + ba states each): step 2 writes the
+// in-vertex candidates into the buffer not holding the wavefront, step 4 merges into the other.
 
 __host__ __device__ inline int64_t al16(int64_t x) { return (x + 15) & ~15LL; }
 
@@ -117,26 +127,20 @@ __host__ __device__ inline WsOff ws_layout(const Caps &c)
 {
 	WsOff o;
 	int64_t p = 0;
-	int64_t na = (int64_t)c.x + c.ba; // merge target of step 4
+	const int64_t na = (int64_t)c.x + c.ba;
 	o.h = p, p = al16(p + 8LL * c.h); // first: 16-byte aligned for vector clears
-	o.a_vd = p, p = al16(p + 8 * na);
-	o.x_vd = p, p = al16(p + 8LL * c.x);
-	o.ba_vd = p, p = al16(p + 8LL * c.ba);
-	o.w0_vd = p, p = al16(p + 8LL * c.w);
-	o.w1_vd = p, p = al16(p + 8LL * c.w);
-	o.n_vd = p, p = al16(p + 8LL * c.w);
+	o.a = p, p = al16(p + 16 * na);
+	o.x = p, p = al16(p + 16 * na);
+	o.ba = p, p = al16(p + 16LL * c.ba);
+	o.w0 = p, p = al16(p + 16LL * c.w);
+	o.w1 = p, p = al16(p + 16LL * c.w);
+	o.nw = p, p = al16(p + 16LL * c.w);
 	o.tb = p, p = al16(p + 8LL * c.tb);
 	o.ta = p, p = al16(p + 8LL * c.ta);
 	o.i0_lo = p, p = al16(p + 8LL * c.iv);
 	o.i0_hi = p, p = al16(p + 8LL * c.iv);
 	o.i1_lo = p, p = al16(p + 8LL * (c.iv + c.tb + c.ta));
 	o.i1_hi = p, p = al16(p + 8LL * (c.iv + c.tb + c.ta));
-	o.a_k = p, p = al16(p + 4 * na);
-	o.x_k = p, p = al16(p + 4LL * c.x);
-	o.ba_k = p, p = al16(p + 4LL * c.ba);
-	o.w0_k = p, p = al16(p + 4LL * c.w);
-	o.w1_k = p, p = al16(p + 4LL * c.w);
-	o.n_k = p, p = al16(p + 4LL * c.w);
 	o.total = al16(p);
 	return o;
 }
@@ -213,12 +217,11 @@ struct ReadCtx {
 // gwf_extend1 (gwf-ed.cu:806-839): last matching offset on diagonal d from offset k. With
 // rc.quirk the start state (k = -1) does not extend when min(ql - d, vl) < 32, as in the
 // reference, whose unsigned max_k disables its serial loop for k = -1.
-__device__ __forceinline__ int32_t ext(const DevGraph &g, const ReadCtx &rc, uint32_t v, int32_t d,
+__device__ __forceinline__ int32_t ext(const DevGraph &g, const ReadCtx &rc, int64_t gb, int32_t d,
                                        int32_t k, int32_t vl)
 {
 	int32_t m = (rc.ql - d < vl ? rc.ql - d : vl) - 1;
 	if (k < 0 && m < 31 && rc.quirk) return k;
-	const int64_t gb = (int64_t)__ldg(g.base + v);
 	if (rc.packed) {
 		for (int guard = 0; k < m && guard < (1 << 26); ++guard) {
 			int32_t rem = m - k;
@@ -248,10 +251,12 @@ __device__ __forceinline__ int32_t ext(const DevGraph &g, const ReadCtx &rc, uin
 }
 
 // q[i] == seq(w)[o] (gwf-ed.cu:1199)
-__device__ __forceinline__ bool base_eq(const DevGraph &g, const ReadCtx &rc, uint32_t w, int32_t o,
+__device__ __forceinline__ int64_t vtx_base(const uint4 &vx) { return (int64_t)((uint64_t)vx.y << 32 | vx.x); }
+
+__device__ __forceinline__ bool base_eq(const DevGraph &g, const ReadCtx &rc, int64_t wb, int32_t o,
                                         int32_t i)
 {
-	const int64_t gp = (int64_t)__ldg(g.base + w) + o;
+	const int64_t gp = wb + o;
 	if (rc.packed) {
 		uint64_t a = __ldg(g.pk + (gp >> 5)) >> ((gp & 31) * 2);
 		uint64_t b = __ldg(rc.qpk + (i >> 5)) >> ((i & 31) * 2);
@@ -297,11 +302,34 @@ __device__ __forceinline__ int32_t upper_bound_u64(const uint64_t *keys, int32_t
 	return lo;
 }
 
-// vd inside one of the sorted disjoint ranges [lo, hi)?
-__device__ __forceinline__ bool in_ranges(const uint64_t *lo, const uint64_t *hi, int32_t n, uint64_t vd)
+// vd inside one of the sorted disjoint ranges [lo, hi)? lo_min / hi_max bound all ranges.
+__device__ __forceinline__ bool in_ranges(const uint64_t *lo, const uint64_t *hi, int32_t n, uint64_t vd,
+                                          uint64_t lo_min, uint64_t hi_max)
 {
+	if (n == 0 || vd < lo_min || vd >= hi_max) return false;
 	int32_t j = upper_bound_u64(lo, n, vd) - 1;
 	return j >= 0 && vd < hi[j];
+}
+
+// Warp bitonic sort of states by vd; the buffer holds pow2ceil(n) entries.
+__device__ inline void warp_bitonic_sort_st(St *a, int32_t n)
+{
+	const int lane = threadIdx.x & 31;
+	if (n <= 1) return;
+	const int32_t N = pow2ceil_i(n);
+	for (int32_t i = n + lane; i < N; i += 32) a[i].vd = PAD_KEY;
+	__syncwarp();
+	for (int32_t k = 2; k <= N; k <<= 1)
+		for (int32_t j = k >> 1; j > 0; j >>= 1) {
+			for (int32_t i = lane; i < N; i += 32) {
+				const int32_t l = i ^ j;
+				if (l > i) {
+					const St x = a[i], y = a[l];
+					if ((x.vd > y.vd) == ((i & k) == 0)) a[i] = y, a[l] = x;
+				}
+			}
+			__syncwarp();
+		}
 }
 
 // Warp bitonic sort of keys[0..n) with int payload; buffers hold pow2ceil(n) entries.

@@ -124,6 +124,7 @@ static std::unordered_map<const gwf_graph_t *, GraphDev *> g_graphs;
 DevGraph GraphDev::view() const
 {
 	DevGraph v;
+	v.vtx = (const uint4 *)vtx.p;
 	v.len = (const uint32_t *)len.p;
 	v.base = (const uint64_t *)base.p;
 	v.pk = (const uint64_t *)pk.p;
@@ -140,7 +141,7 @@ GraphDev::~GraphDev()
 	int cur = -1;
 	cudaGetDevice(&cur);
 	if (device >= 0) cudaSetDevice(device);
-	len.release(), base.release(), pk.release(), raw.release(), arc_off.release(), arc.release();
+	vtx.release(), len.release(), base.release(), pk.release(), raw.release(), arc_off.release(), arc.release();
 	if (cur >= 0) cudaSetDevice(cur);
 }
 
@@ -177,17 +178,22 @@ static int upload_graph(const gwf_graph_t *g, GraphDev *G)
 	std::vector<uint32_t> off(nv + 1, 0);
 	for (uint32_t e = 0; e < g->n_arc; ++e) off[(uint32_t)(g->arc[e].a >> 32) + 1]++;
 	for (uint32_t v = 0; v < nv; ++v) off[v + 1] += off[v];
+	std::vector<uint4> vtx(nv ? nv : 1);
+	for (uint32_t v = 0; v < nv; ++v)
+		vtx[v] = make_uint4((uint32_t)base[v], (uint32_t)(base[v] >> 32), len[v], off[v]);
 	std::vector<uint2> arc(g->n_arc ? g->n_arc : 1);
 	for (uint32_t e = 0; e < g->n_arc; ++e) arc[e] = make_uint2((uint32_t)g->arc[e].a, (uint32_t)g->arc[e].o);
 	G->n_vtx = nv, G->n_arc = g->n_arc, G->pure = pure, G->total_len = tot;
 	G->dens_milli = (int32_t)std::max<uint64_t>(1, (uint64_t)nv * 1000 / std::max<uint64_t>(1, tot));
 	int rc;
+	if ((rc = G->vtx.ensure(sizeof(uint4) * vtx.size()))) return rc;
 	if ((rc = G->len.ensure(sizeof(uint32_t) * std::max<size_t>(nv, 1)))) return rc;
 	if ((rc = G->base.ensure(sizeof(uint64_t) * std::max<size_t>(nv, 1)))) return rc;
 	if ((rc = G->pk.ensure(sizeof(uint64_t) * nw))) return rc;
 	if ((rc = G->raw.ensure(raw.size()))) return rc;
 	if ((rc = G->arc_off.ensure(sizeof(uint32_t) * (nv + 1)))) return rc;
 	if ((rc = G->arc.ensure(sizeof(uint2) * arc.size()))) return rc;
+	CK(cudaMemcpy(G->vtx.p, vtx.data(), sizeof(uint4) * vtx.size(), cudaMemcpyHostToDevice));
 	CK(cudaMemcpy(G->len.p, len.data(), sizeof(uint32_t) * nv, cudaMemcpyHostToDevice));
 	CK(cudaMemcpy(G->base.p, base.data(), sizeof(uint64_t) * nv, cudaMemcpyHostToDevice));
 	CK(cudaMemcpy(G->pk.p, pk.data(), sizeof(uint64_t) * nw, cudaMemcpyHostToDevice));

@@ -27,7 +27,7 @@ struct GraphDev { // device-resident copy of one gwf_graph_t
 	uint32_t n_vtx = 0, n_arc = 0;
 	int32_t pure = 0, dens_milli = 1;
 	uint64_t total_len = 0;
-	DBuf len, base, pk, raw, arc_off, arc;
+	DBuf vtx, len, base, pk, raw, arc_off, arc;
 	gwfb::DevGraph view() const;
 	~GraphDev();
 };
