@@ -34,7 +34,6 @@ constexpr int32_t ST_BAD_INPUT = -2;
 constexpr int32_t ST_CAPACITY = -4;
 
 struct DevGraph {
-	const uint4 *vtx;        // [n_vtx] (base low 32 bits, base high 32 bits, length, first arc)
 	const uint32_t *len;     // [n_vtx]
 	const uint64_t *base;    // [n_vtx] first base of the vertex in the concatenated sequence
 	const uint64_t *pk;      // 2-bit packed sequence, 32 bases per word, +2 padding words
@@ -55,14 +54,6 @@ struct DevReads {
 	const uint8_t *pure;    // 1 when the read is A/C/G/T only
 	int32_t v1;
 	int32_t n;
-};
-
-// One wavefront state: diagonal vd and offset k of the last matched base (16 bytes, one vector
-// load or store).
-struct __align__(16) St {
-	uint64_t vd;
-	int32_t k;
-	int32_t pad;
 };
 
 // Per-warp arena capacities (entries).
@@ -116,10 +107,11 @@ __host__ __device__ inline Caps caps_for(int32_t ql, int32_t level, int32_t dens
 }
 
 struct WsOff { // byte offsets in one warp arena
-	int64_t h, a, x, ba, w0, w1, nw, tb, ta, i0_lo, i0_hi, i1_lo, i1_hi, total;
+	int64_t a_vd, a_k, x_vd, x_k, ba_vd, ba_k, w0_vd, w0_k, w1_vd, w1_k, n_vd, n_k, tb, ta, i0_lo,
+	    i0_hi, i1_lo, i1_hi, h, total;
 };
-// The wavefront ping-pongs between the a and x buffers (x + ba states each): step 2 writes the
-// in-vertex candidates into the buffer not holding the wavefront, step 4 merges into the other.
+// The wavefront ping-pongs between the a and x buffers (each x + ba entries): step 2 writes the
+// in-vertex candidates into the buffer not holding the wavefront.
 
 __host__ __device__ inline int64_t al16(int64_t x) { return (x + 15) & ~15LL; }
 
@@ -127,20 +119,26 @@ __host__ __device__ inline WsOff ws_layout(const Caps &c)
 {
 	WsOff o;
 	int64_t p = 0;
-	const int64_t na = (int64_t)c.x + c.ba;
+	int64_t na = (int64_t)c.x + c.ba; // merge target of step 4
 	o.h = p, p = al16(p + 8LL * c.h); // first: 16-byte aligned for vector clears
-	o.a = p, p = al16(p + 16 * na);
-	o.x = p, p = al16(p + 16 * na);
-	o.ba = p, p = al16(p + 16LL * c.ba);
-	o.w0 = p, p = al16(p + 16LL * c.w);
-	o.w1 = p, p = al16(p + 16LL * c.w);
-	o.nw = p, p = al16(p + 16LL * c.w);
+	o.a_vd = p, p = al16(p + 8 * na);
+	o.x_vd = p, p = al16(p + 8 * na);
+	o.ba_vd = p, p = al16(p + 8LL * c.ba);
+	o.w0_vd = p, p = al16(p + 8LL * c.w);
+	o.w1_vd = p, p = al16(p + 8LL * c.w);
+	o.n_vd = p, p = al16(p + 8LL * c.w);
 	o.tb = p, p = al16(p + 8LL * c.tb);
 	o.ta = p, p = al16(p + 8LL * c.ta);
 	o.i0_lo = p, p = al16(p + 8LL * c.iv);
 	o.i0_hi = p, p = al16(p + 8LL * c.iv);
 	o.i1_lo = p, p = al16(p + 8LL * (c.iv + c.tb + c.ta));
 	o.i1_hi = p, p = al16(p + 8LL * (c.iv + c.tb + c.ta));
+	o.a_k = p, p = al16(p + 4 * na);
+	o.x_k = p, p = al16(p + 4 * na);
+	o.ba_k = p, p = al16(p + 4LL * c.ba);
+	o.w0_k = p, p = al16(p + 4LL * c.w);
+	o.w1_k = p, p = al16(p + 4LL * c.w);
+	o.n_k = p, p = al16(p + 4LL * c.w);
 	o.total = al16(p);
 	return o;
 }
@@ -214,29 +212,47 @@ struct ReadCtx {
 	bool quirk;           // reference start-state rules (ext, and the k=-1 filter of step 2)
 };
 
+// 32 bases starting at base position pos of a 2-bit packed sequence, as (lo, hi) 16-base
+// halves: three aligned 32-bit loads and two funnel shifts (the arrays carry padding words).
+__device__ __forceinline__ void window32(const uint32_t *__restrict__ pk, int64_t pos, uint32_t &lo,
+                                        uint32_t &hi)
+{
+	const uint32_t *w = pk + (pos >> 4);
+	const uint32_t sh = (uint32_t)(pos & 15) * 2;
+	const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+	lo = __funnelshift_r(w0, w1, sh);
+	hi = __funnelshift_r(w1, w2, sh);
+}
+
 // gwf_extend1 (gwf-ed.cu:806-839): last matching offset on diagonal d from offset k. With
 // rc.quirk the start state (k = -1) does not extend when min(ql - d, vl) < 32, as in the
 // reference, whose unsigned max_k disables its serial loop for k = -1.
-__device__ __forceinline__ int32_t ext(const DevGraph &g, const ReadCtx &rc, int64_t gb, int32_t d,
+__device__ __forceinline__ int32_t ext(const DevGraph &g, const ReadCtx &rc, uint32_t v, int32_t d,
                                        int32_t k, int32_t vl)
 {
-	int32_t m = (rc.ql - d < vl ? rc.ql - d : vl) - 1;
+	const int32_t m = (rc.ql - d < vl ? rc.ql - d : vl) - 1;
 	if (k < 0 && m < 31 && rc.quirk) return k;
+	const int64_t gb = (int64_t)__ldg(g.base + v);
 	if (rc.packed) {
+		const uint32_t *gp = (const uint32_t *)g.pk, *qp = (const uint32_t *)rc.qpk;
 		for (int guard = 0; k < m && guard < (1 << 26); ++guard) {
-			int32_t rem = m - k;
-			uint64_t x = window2(g.pk, gb + k + 1) ^ window2(rc.qpk, (int64_t)d + k + 1);
-			if (rem < 32) x |= ~0ULL << (2 * rem);
-			if (x == 0) {
+			uint32_t glo, ghi, qlo, qhi;
+			window32(gp, gb + k + 1, glo, ghi);
+			window32(qp, (int64_t)d + k + 1, qlo, qhi);
+			uint32_t xlo = glo ^ qlo, xhi = ghi ^ qhi;
+			const int32_t rem = m - k; // bases left to compare, >= 1
+			if (rem < 16) xlo |= ~0u << (2 * rem), xhi = ~0u;
+			else if (rem < 32) xhi |= (rem == 16 ? ~0u : ~0u << (2 * (rem - 16)));
+			if ((xlo | xhi) == 0) {
 				k += 32;
 				continue;
 			}
-			k += __ffsll((long long)x) - 1 >> 1;
+			k += xlo ? (__ffs(xlo) - 1) >> 1 : 16 + ((__ffs(xhi) - 1) >> 1);
 			break;
 		}
 	} else {
 		for (int guard = 0; k < m && guard < (1 << 28); ++guard) {
-			int32_t rem = m - k;
+			const int32_t rem = m - k;
 			uint64_t x = window8(g.raw, gb + k + 1) ^ window8(rc.qraw, (int64_t)d + k + 1);
 			if (rem < 8) x |= ~0ULL << (8 * rem);
 			if (x == 0) {
@@ -251,12 +267,10 @@ __device__ __forceinline__ int32_t ext(const DevGraph &g, const ReadCtx &rc, int
 }
 
 // q[i] == seq(w)[o] (gwf-ed.cu:1199)
-__device__ __forceinline__ int64_t vtx_base(const uint4 &vx) { return (int64_t)((uint64_t)vx.y << 32 | vx.x); }
-
-__device__ __forceinline__ bool base_eq(const DevGraph &g, const ReadCtx &rc, int64_t wb, int32_t o,
+__device__ __forceinline__ bool base_eq(const DevGraph &g, const ReadCtx &rc, uint32_t w, int32_t o,
                                         int32_t i)
 {
-	const int64_t gp = wb + o;
+	const int64_t gp = (int64_t)__ldg(g.base + w) + o;
 	if (rc.packed) {
 		uint64_t a = __ldg(g.pk + (gp >> 5)) >> ((gp & 31) * 2);
 		uint64_t b = __ldg(rc.qpk + (i >> 5)) >> ((i & 31) * 2);
@@ -309,27 +323,6 @@ __device__ __forceinline__ bool in_ranges(const uint64_t *lo, const uint64_t *hi
 	if (n == 0 || vd < lo_min || vd >= hi_max) return false;
 	int32_t j = upper_bound_u64(lo, n, vd) - 1;
 	return j >= 0 && vd < hi[j];
-}
-
-// Warp bitonic sort of states by vd; the buffer holds pow2ceil(n) entries.
-__device__ inline void warp_bitonic_sort_st(St *a, int32_t n)
-{
-	const int lane = threadIdx.x & 31;
-	if (n <= 1) return;
-	const int32_t N = pow2ceil_i(n);
-	for (int32_t i = n + lane; i < N; i += 32) a[i].vd = PAD_KEY;
-	__syncwarp();
-	for (int32_t k = 2; k <= N; k <<= 1)
-		for (int32_t j = k >> 1; j > 0; j >>= 1) {
-			for (int32_t i = lane; i < N; i += 32) {
-				const int32_t l = i ^ j;
-				if (l > i) {
-					const St x = a[i], y = a[l];
-					if ((x.vd > y.vd) == ((i & k) == 0)) a[i] = y, a[l] = x;
-				}
-			}
-			__syncwarp();
-		}
 }
 
 // Warp bitonic sort of keys[0..n) with int payload; buffers hold pow2ceil(n) entries.

@@ -34,12 +34,18 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 	const DevGraph &g = p.g;
 	const WsOff o = ws_layout(c);
 	uint64_t *const h = (uint64_t *)(wsb + o.h);
-	St *A = (St *)(wsb + o.a);   // wavefront
-	St *X = (St *)(wsb + o.x);   // next wavefront being built
-	St *const BA = (St *)(wsb + o.ba);
-	St *E = (St *)(wsb + o.w0);  // current wave of vertex-end states
-	St *F = (St *)(wsb + o.w1);  // next wave
-	St *const NW = (St *)(wsb + o.nw); // states entered with a free match
+	uint64_t *a_vd = (uint64_t *)(wsb + o.a_vd);
+	int32_t *a_k = (int32_t *)(wsb + o.a_k);
+	uint64_t *x_vd = (uint64_t *)(wsb + o.x_vd);
+	int32_t *x_k = (int32_t *)(wsb + o.x_k);
+	uint64_t *const ba_vd = (uint64_t *)(wsb + o.ba_vd);
+	int32_t *const ba_k = (int32_t *)(wsb + o.ba_k);
+	uint64_t *e_vd = (uint64_t *)(wsb + o.w0_vd);
+	int32_t *e_k = (int32_t *)(wsb + o.w0_k);
+	uint64_t *f_vd = (uint64_t *)(wsb + o.w1_vd);
+	int32_t *f_k = (int32_t *)(wsb + o.w1_k);
+	uint64_t *const n_vd = (uint64_t *)(wsb + o.n_vd);
+	int32_t *const n_k = (int32_t *)(wsb + o.n_k);
 	uint64_t *const tb = (uint64_t *)(wsb + o.tb);
 	uint64_t *const ta = (uint64_t *)(wsb + o.ta);
 	uint64_t *const ilo = (uint64_t *)(wsb + o.i0_lo);
@@ -70,11 +76,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 		const uint4 z = make_uint4(0, 0, 0, 0);
 		for (int32_t i = lane; i < c.h / 2; i += 32) h4[i] = z;
 	}
-	if (lane == 0) {
-		St s0;
-		s0.vd = gen_vd((uint32_t)v0, 0), s0.k = -1, s0.pad = 0; // gwf-ed.cu:1303-1308
-		A[0] = s0;
-	}
+	if (lane == 0) a_vd[0] = gen_vd((uint32_t)v0, 0), a_k[0] = -1; // gwf-ed.cu:1303-1308
 	__syncwarp();
 	const uint32_t hmask = (uint32_t)c.h - 1;
 	const int32_t hlimit = c.h - c.h / 4;
@@ -90,76 +92,56 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 		W += n_a;
 		bool found = false, ovf = false;
 
-		// ---- phases 1+2, one pipelined pass over the wavefront: extend every diagonal
-		// (gwf-ed.cu:902-910, 806-839), collect vertex-end states into the first wave
-		// (gwf-ed.cu:965-984), and emit the in-vertex successors (gwf-ed.cu:912-1016) from
-		// registers; the chunk after the current one is extended first, so lane 31 can read the
-		// extended k of its right neighbour.
-		int32_t n_e = 0, n_x = 0, n_tb = 0;
-		uint64_t c_vd = 0;
-		int32_t c_k = 0, c_vl = 0;
-		{
-			const int32_t j = lane;
-			if (j < n_a) {
-				const St e = A[j];
-				const uint4 vx = __ldg(g.vtx + vd_v(e.vd));
-				c_vd = e.vd, c_vl = (int32_t)vx.z;
-				c_k = ext(g, rc, vtx_base(vx), vd_d(e.vd), e.k, c_vl);
-			}
-		}
-		uint64_t carry_vd = 0;
-		int32_t carry_k = 0;
+		// ---- phase 1: extend every diagonal; collect vertex-end (and, for v1 >= 0,
+		// query-end) states into the first wave (gwf-ed.cu:902-910, 965-984)
+		int32_t n_e = 0;
 		for (int32_t base = 0; base < n_a; base += 32) {
 			const int32_t j = base + lane;
-			const bool act = j < n_a;
-			uint64_t n_vd = 0;
-			int32_t n_k = 0, n_vl = 0;
-			if (base + 32 < n_a) {
-				const int32_t jn = base + 32 + lane;
-				if (jn < n_a) {
-					const St e = A[jn];
-					const uint4 vx = __ldg(g.vtx + vd_v(e.vd));
-					n_vd = e.vd, n_vl = (int32_t)vx.z;
-					n_k = ext(g, rc, vtx_base(vx), vd_d(e.vd), e.k, n_vl);
-				}
-			}
-			// classification
-			const uint32_t v = vd_v(c_vd);
-			const int32_t d = vd_d(c_vd);
 			bool toE = false;
-			if (act) {
-				const bool vend = c_k == c_vl - 1, qend = d + c_k == ql - 1;
+			uint64_t vd = 0;
+			int32_t k = 0;
+			if (j < n_a) {
+				vd = a_vd[j];
+				k = a_k[j];
+				const uint32_t v = vd_v(vd);
+				const int32_t d = vd_d(vd), vl = (int32_t)__ldg(g.len + v);
+				k = ext(g, rc, v, d, k, vl);
+				a_k[j] = k;
+				const bool vend = k == vl - 1, qend = d + k == ql - 1;
 				if (qend) {
 					if (v1 < 0 || ((int32_t)v == v1 && vend)) found = true;
 					else toE = true;
 				} else if (vend)
 					toE = true;
 			}
-			{
-				const uint32_t m = __ballot_sync(FULL, toE);
-				const int32_t pos = n_e + __popc(m & lanemask_lt());
-				if (toE && pos < c.w) {
-					St e;
-					e.vd = c_vd, e.k = c_k, e.pad = 0;
-					E[pos] = e;
-				}
-				n_e += __popc(m);
-			}
-			// neighbours: previous from the carry, next from the pipelined chunk
-			uint64_t pv = __shfl_up_sync(FULL, c_vd, 1);
-			int32_t pk = __shfl_up_sync(FULL, c_k, 1);
-			uint64_t nv = __shfl_down_sync(FULL, c_vd, 1);
-			int32_t nk = __shfl_down_sync(FULL, c_k, 1);
-			const uint64_t f_vd = __shfl_sync(FULL, n_vd, 0);
-			const int32_t f_k = __shfl_sync(FULL, n_k, 0);
-			if (lane == 0) pv = carry_vd, pk = carry_k;
-			if (lane == 31) nv = f_vd, nk = f_k;
+			const uint32_t m = __ballot_sync(FULL, toE);
+			const int32_t pos = n_e + __popc(m & lanemask_lt());
+			if (toE && pos < c.w) e_vd[pos] = vd, e_k[pos] = k;
+			n_e += __popc(m);
+		}
+		if (__any_sync(FULL, found)) {
+			dist = s;
+			break;
+		}
+		if (n_e > c.w) ovf = true;
+		__syncwarp();
+
+		// ---- phase 2: in-vertex successors, sorted and unique by construction
+		// (gwf_ed_extend_batch, gwf-ed.cu:912-1016)
+		int32_t n_x = 0, n_tb = 0;
+		for (int32_t base = 0; base < n_a; base += 32) {
+			const int32_t j = base + lane;
 			uint64_t cv[3];
 			int32_t ck[3];
 			bool keep[3] = {false, false, false}, tmp[3] = {false, false, false};
-			if (act) {
-				const uint64_t vd = c_vd;
-				const int32_t k = c_k, vl = c_vl;
+			if (j < n_a) {
+				const uint64_t vd = a_vd[j];
+				const int32_t k = a_k[j];
+				const int32_t vl = (int32_t)__ldg(g.len + vd_v(vd));
+				const uint64_t pv = j > 0 ? a_vd[j - 1] : 0;
+				const int32_t pk = j > 0 ? a_k[j - 1] : 0;
+				const uint64_t nv = j + 1 < n_a ? a_vd[j + 1] : 0;
+				const int32_t nk = j + 1 < n_a ? a_k[j + 1] : 0;
 				const bool left_in = j > 0 && pv == vd - 1, left2 = j > 0 && pv == vd - 2;
 				const bool right_in = j + 1 < n_a && nv == vd + 1, right2 = j + 1 < n_a && nv == vd + 2;
 				bool has[3];
@@ -179,48 +161,43 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				cv[2] = vd + 1;
 				ck[2] = k;
 				// the reference keeps vl in a uint32_t here (gwf-ed.cu:895, 993): a candidate
-				// with k = -1 (insertion before the first base of v0) fails `k < vl` and is
-				// dropped. Diagonals that already ended their vertex are dropped now (the
-				// intervals only grow; step 4 re-filters when this step adds intervals).
+				// with k = -1 (insertion before the first base of v0) fails `k < vl` and is dropped
 #pragma unroll
 				for (int t = 0; t < 3; ++t)
 					if (has[t]) {
 						const int32_t dd = vd_d(cv[t]);
 						const bool kin = rc.quirk ? (uint32_t)ck[t] < (uint32_t)vl : ck[t] < vl;
-						if (dd + ck[t] < ql && kin) keep[t] = !in_ranges(ilo, ihi, n_i, cv[t], i_min, i_max);
+						if (dd + ck[t] < ql && kin) keep[t] = true;
 						else if (ck[t] == vl) tmp[t] = true;
 					}
 			}
-			int32_t tot, tott;
-			const int32_t nkeep = (int32_t)keep[0] + keep[1] + keep[2];
-			const int32_t ntmp = (int32_t)tmp[0] + tmp[1] + tmp[2];
-			int32_t off = warp_excl_scan(nkeep, &tot) + n_x;
-			int32_t offt = warp_excl_scan(ntmp, &tott) + n_tb;
+			{
+				const uint32_t lt = lanemask_lt();
+				const uint32_t k0 = __ballot_sync(FULL, keep[0]), k1 = __ballot_sync(FULL, keep[1]),
+				               k2 = __ballot_sync(FULL, keep[2]);
+				int32_t off = n_x + __popc(k0 & lt) + __popc(k1 & lt) + __popc(k2 & lt);
 #pragma unroll
-			for (int t = 0; t < 3; ++t) {
-				if (keep[t]) {
-					if (off < c.x) {
-						St e;
-						e.vd = cv[t], e.k = ck[t], e.pad = 0;
-						X[off] = e;
+				for (int t = 0; t < 3; ++t)
+					if (keep[t]) {
+						if (off < c.x) x_vd[off] = cv[t], x_k[off] = ck[t];
+						++off;
 					}
-					++off;
-				}
-				if (tmp[t]) {
-					if (offt < c.tb) tb[offt] = cv[t];
-					++offt;
+				n_x += __popc(k0) + __popc(k1) + __popc(k2);
+				const uint32_t t0 = __ballot_sync(FULL, tmp[0]), t1 = __ballot_sync(FULL, tmp[1]),
+				               t2 = __ballot_sync(FULL, tmp[2]);
+				if (t0 | t1 | t2) {
+					int32_t offt = n_tb + __popc(t0 & lt) + __popc(t1 & lt) + __popc(t2 & lt);
+#pragma unroll
+					for (int t = 0; t < 3; ++t)
+						if (tmp[t]) {
+							if (offt < c.tb) tb[offt] = cv[t];
+							++offt;
+						}
+					n_tb += __popc(t0) + __popc(t1) + __popc(t2);
 				}
 			}
-			n_x += tot, n_tb += tott;
-			carry_vd = __shfl_sync(FULL, c_vd, 31);
-			carry_k = __shfl_sync(FULL, c_k, 31);
-			c_vd = n_vd, c_k = n_k, c_vl = n_vl;
 		}
-		if (__any_sync(FULL, found)) {
-			dist = s;
-			break;
-		}
-		if (n_e > c.w || n_x > c.x || n_tb > c.tb) ovf = true;
+		if (n_x > c.x || n_tb > c.tb) ovf = true;
 		__syncwarp();
 
 		// ---- phase 3: vertex-end states over arcs, in waves until no state is entered with a
@@ -234,18 +211,16 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 			int32_t n_n = 0;
 			for (int32_t base = 0; base < n_e; base += 32) {
 				const int32_t j = base + lane;
-				bool isq = false, isv = false;
+				bool act = j < n_e, isq = false, isv = false;
 				uint64_t vd = 0;
 				int32_t k = 0, d = 0, vl = 0, i = 0, nv = 0;
 				uint32_t v = 0, aoff = 0;
-				if (j < n_e) {
-					const St e = E[j];
-					vd = e.vd, k = e.k;
-					v = vd_v(vd), d = vd_d(vd), i = d + k;
-					const uint4 vx = __ldg(g.vtx + v);
-					vl = (int32_t)vx.z, aoff = vx.w;
+				if (act) {
+					vd = e_vd[j], k = e_k[j];
+					v = vd_v(vd), d = vd_d(vd), vl = (int32_t)__ldg(g.len + v), i = d + k;
 					isq = i == ql - 1;
 					isv = !isq;
+					aoff = __ldg(g.arc_off + v);
 					const int32_t deg = (int32_t)(__ldg(g.arc_off + v + 1) - aoff);
 					if (isv || (k + 1 == vl && (int32_t)v != v1)) nv = deg;
 				}
@@ -269,7 +244,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 							const int ins = hset_insert(h, hmask, (uint64_t)w << 32 | (uint32_t)(i + 1));
 							if (ins < 0) ovf = true;
 							const bool absent = ins == 1;
-							if (base_eq(g, rc, vtx_base(__ldg(g.vtx + w)), ol, i + 1)) {
+							if (base_eq(g, rc, w, ol, i + 1)) {
 								++n_ext;
 								enter = absent;
 							} else
@@ -280,28 +255,17 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 					}
 					const uint32_t me = __ballot_sync(FULL, enter);
 					const int32_t pe = n_n + __popc(me & lanemask_lt());
-					if (enter && pe < c.w) {
-						St e;
-						e.vd = gen_vd(w, i + 1 - ol), e.k = ol, e.pad = 0;
-						NW[pe] = e;
-					}
+					if (enter && pe < c.w) n_vd[pe] = gen_vd(w, i + 1 - ol), n_k[pe] = ol;
 					n_n += __popc(me);
 					int32_t tot;
-					const int32_t pb = warp_excl_scan(two ? 2 : (one ? 1 : 0), &tot) + n_ba;
+					int32_t pb = warp_excl_scan(two ? 2 : (one ? 1 : 0), &tot) + n_ba;
 					if (two) {
 						if (pb + 1 < c.ba) {
-							St e;
-							e.vd = gen_vd(w, i - ol), e.k = ol, e.pad = 0; // deletion
-							BA[pb] = e;
-							e.vd = gen_vd(w, i + 1 - ol); // mismatch
-							BA[pb + 1] = e;
+							ba_vd[pb] = gen_vd(w, i - ol), ba_k[pb] = ol;         // deletion
+							ba_vd[pb + 1] = gen_vd(w, i + 1 - ol), ba_k[pb + 1] = ol; // mismatch
 						}
 					} else if (one) {
-						if (pb < c.ba) {
-							St e;
-							e.vd = gen_vd(w, i - ol), e.k = ol, e.pad = 0;
-							BA[pb] = e;
-						}
+						if (pb < c.ba) ba_vd[pb] = gen_vd(w, i - ol), ba_k[pb] = ol;
 					}
 					n_ba += tot;
 				}
@@ -312,10 +276,8 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				const uint32_t mi = __ballot_sync(FULL, ins || qdel);
 				const int32_t pi = n_ba + __popc(mi & lanemask_lt());
 				if ((ins || qdel) && pi < c.ba) {
-					St e;
-					e.vd = ins ? gen_vd(v, d + 1) : gen_vd(v, d - 1);
-					e.k = ins ? k : k + 1, e.pad = 0;
-					BA[pi] = e;
+					ba_vd[pi] = ins ? gen_vd(v, d + 1) : gen_vd(v, d - 1);
+					ba_k[pi] = ins ? k : k + 1;
 				}
 				n_ba += __popc(mi);
 			}
@@ -339,12 +301,10 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				int32_t k = 0, d = 0;
 				uint32_t v = 0;
 				if (j < n_n) {
-					const St e = NW[j];
-					vd = e.vd, k = e.k;
+					vd = n_vd[j], k = n_k[j];
 					v = vd_v(vd), d = vd_d(vd);
-					const uint4 vx = __ldg(g.vtx + v);
-					const int32_t vl = (int32_t)vx.z;
-					k = ext(g, rc, vtx_base(vx), d, k, vl);
+					const int32_t vl = (int32_t)__ldg(g.len + v);
+					k = ext(g, rc, v, d, k, vl);
 					const int32_t i = d + k;
 					if (i == ql - 1) {
 						if (v1 < 0 || ((int32_t)v == v1 && k == vl - 1)) found = true;
@@ -356,23 +316,14 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				}
 				const uint32_t mf = __ballot_sync(FULL, toF);
 				const int32_t pf = n_f + __popc(mf & lanemask_lt());
-				if (toF && pf < c.w) {
-					St e;
-					e.vd = vd, e.k = k, e.pad = 0;
-					F[pf] = e;
-				}
+				if (toF && pf < c.w) f_vd[pf] = vd, f_k[pf] = k;
 				n_f += __popc(mf);
 				const uint32_t m3 = __ballot_sync(FULL, three);
 				const int32_t p3 = n_ba + 3 * __popc(m3 & lanemask_lt());
 				if (three && p3 + 2 < c.ba) {
-					St e;
-					e.pad = 0;
-					e.vd = gen_vd(v, d - 1), e.k = k + 1; // deletion
-					BA[p3] = e;
-					e.vd = gen_vd(v, d), e.k = k + 1; // mismatch
-					BA[p3 + 1] = e;
-					e.vd = gen_vd(v, d + 1), e.k = k; // insertion
-					BA[p3 + 2] = e;
+					ba_vd[p3] = gen_vd(v, d - 1), ba_k[p3] = k + 1;     // deletion
+					ba_vd[p3 + 1] = gen_vd(v, d), ba_k[p3 + 1] = k + 1; // mismatch
+					ba_vd[p3 + 2] = gen_vd(v, d + 1), ba_k[p3 + 2] = k; // insertion
 				}
 				n_ba += 3 * __popc(m3);
 			}
@@ -382,8 +333,9 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				break;
 			}
 			__syncwarp();
-			St *t = E;
-			E = F, F = t;
+			uint64_t *tv = e_vd;
+			int32_t *tk = e_k;
+			e_vd = f_vd, e_k = f_k, f_vd = tv, f_k = tk;
 			n_e = n_f;
 		}
 		if (__any_sync(FULL, found)) {
@@ -398,8 +350,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 
 		// ---- phase 4: ended-diagonal intervals, then the next wavefront
 		// (gwf_dedup / gwf_intv_merge2 / gwf_diag_dedup / gwf_mixed_dedup, gwf-ed.cu:780-804)
-		const bool new_intervals = n_tb + n_ta > 0;
-		if (new_intervals) {
+		if (n_tb + n_ta > 0) {
 			warp_bitonic_sort(ta, nullptr, n_ta);
 			// rank-merge the old ranges with both point lists, ties ordered I < TB < TA
 			const int32_t n_c = n_i + n_tb + n_ta;
@@ -458,69 +409,65 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 		}
 		int32_t n_new = 0;
 		if (n_ba == 0) {
-			// only in-vertex candidates: sorted, unique and filtered against the previous
-			// intervals; re-filter in place when this step added intervals
-			if (new_intervals) {
-				for (int32_t base = 0; base < n_x; base += 32) {
-					const int32_t j = base + lane;
-					St e;
-					bool keep = false;
-					if (j < n_x) {
-						e = X[j];
-						keep = !in_ranges(ilo, ihi, n_i, e.vd, i_min, i_max);
-					}
-					const uint32_t m = __ballot_sync(FULL, keep);
-					if (keep) X[n_new + __popc(m & lanemask_lt())] = e;
-					n_new += __popc(m);
+			// only in-vertex candidates: already sorted and unique; drop ended diagonals in place
+			// and make the candidate buffer the wavefront
+			for (int32_t base = 0; base < n_x; base += 32) {
+				const int32_t j = base + lane;
+				uint64_t vd = 0;
+				int32_t k = 0;
+				bool keep = false;
+				if (j < n_x) {
+					vd = x_vd[j], k = x_k[j];
+					keep = !in_ranges(ilo, ihi, n_i, vd, i_min, i_max);
 				}
-			} else
-				n_new = n_x;
-			St *t = A;
-			A = X, X = t;
+				const uint32_t m = __ballot_sync(FULL, keep);
+				if (keep) {
+					const int32_t pos = n_new + __popc(m & lanemask_lt());
+					x_vd[pos] = vd, x_k[pos] = k;
+				}
+				n_new += __popc(m);
+			}
+			uint64_t *tv = a_vd;
+			int32_t *tk = a_k;
+			a_vd = x_vd, a_k = x_k, x_vd = tv, x_k = tk;
 			__syncwarp();
 		} else {
-			warp_bitonic_sort_st(BA, n_ba);
-			// merge the in-vertex and arc-side candidates into the free buffer (ties: in-vertex
-			// first), keep the furthest k per diagonal and drop ended diagonals
+			warp_bitonic_sort(ba_vd, ba_k, n_ba);
+			// merge the in-vertex and arc-side candidates into a (ties: in-vertex first)
 			const int32_t n_m = n_x + n_ba;
 			for (int32_t j = lane; j < n_x; j += 32) {
-				const St e = X[j];
-				int32_t lo = 0, hi = n_ba;
-				while (lo < hi) {
-					const int32_t mid = (lo + hi) >> 1;
-					if (BA[mid].vd < e.vd) lo = mid + 1; else hi = mid;
-				}
-				A[j + lo] = e;
+				const uint64_t x = x_vd[j];
+				const int32_t pos = j + lower_bound_u64(ba_vd, n_ba, x);
+				a_vd[pos] = x, a_k[pos] = x_k[j];
 			}
 			for (int32_t j = lane; j < n_ba; j += 32) {
-				const St e = BA[j];
-				int32_t lo = 0, hi = n_x;
-				while (lo < hi) {
-					const int32_t mid = (lo + hi) >> 1;
-					if (X[mid].vd <= e.vd) lo = mid + 1; else hi = mid;
-				}
-				A[j + lo] = e;
+				const uint64_t x = ba_vd[j];
+				const int32_t pos = j + upper_bound_u64(x_vd, n_x, x);
+				a_vd[pos] = x, a_k[pos] = ba_k[j];
 			}
 			__syncwarp();
+			// keep the furthest k per diagonal, drop diagonals inside an ended interval
 			for (int32_t base = 0; base < n_m; base += 32) {
 				const int32_t j = base + lane;
 				bool keep = false;
-				St e;
-				e.vd = 0, e.k = 0, e.pad = 0;
+				uint64_t vd = 0;
+				int32_t k = 0;
 				if (j < n_m) {
-					e = A[j];
-					if (j == 0 || A[j - 1].vd != e.vd) {
-						for (int32_t t = j + 1; t < n_m; ++t) {
-							const St f = A[t];
-							if (f.vd != e.vd) break;
-							e.k = f.k > e.k ? f.k : e.k;
+					vd = a_vd[j], k = a_k[j];
+					if (j == 0 || a_vd[j - 1] != vd) {
+						for (int32_t t = j + 1; t < n_m && a_vd[t] == vd; ++t) {
+							const int32_t kt = a_k[t];
+							k = kt > k ? kt : k;
 						}
-						keep = !in_ranges(ilo, ihi, n_i, e.vd, i_min, i_max);
+						keep = !in_ranges(ilo, ihi, n_i, vd, i_min, i_max);
 					}
 				}
 				__syncwarp();
 				const uint32_t m = __ballot_sync(FULL, keep);
-				if (keep) A[n_new + __popc(m & lanemask_lt())] = e;
+				if (keep) {
+					const int32_t pos = n_new + __popc(m & lanemask_lt());
+					a_vd[pos] = vd, a_k[pos] = k;
+				}
 				n_new += __popc(m);
 				__syncwarp();
 			}
@@ -545,7 +492,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 }
 
 // Plain form: one warp per queue position, arena offsets per read (main.cu:151-236 layout).
-__global__ void __launch_bounds__(256, 4) k_align_plain(const __grid_constant__ KParams p)
+__global__ void __launch_bounds__(256, 3) k_align_plain(const __grid_constant__ KParams p)
 {
 	const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
 	if (gw >= p.n_order) return;
@@ -555,7 +502,7 @@ __global__ void __launch_bounds__(256, 4) k_align_plain(const __grid_constant__ 
 }
 
 // Persistent form: each warp owns one arena and pulls reads from the cost-ordered queue.
-__global__ void __launch_bounds__(256, 4) k_align_persistent(const __grid_constant__ KParams p)
+__global__ void __launch_bounds__(256, 3) k_align_persistent(const __grid_constant__ KParams p)
 {
 	const int lane = threadIdx.x & 31;
 	const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);

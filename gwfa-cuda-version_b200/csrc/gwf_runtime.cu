@@ -124,7 +124,6 @@ static std::unordered_map<const gwf_graph_t *, GraphDev *> g_graphs;
 DevGraph GraphDev::view() const
 {
 	DevGraph v;
-	v.vtx = (const uint4 *)vtx.p;
 	v.len = (const uint32_t *)len.p;
 	v.base = (const uint64_t *)base.p;
 	v.pk = (const uint64_t *)pk.p;
@@ -141,7 +140,7 @@ GraphDev::~GraphDev()
 	int cur = -1;
 	cudaGetDevice(&cur);
 	if (device >= 0) cudaSetDevice(device);
-	vtx.release(), len.release(), base.release(), pk.release(), raw.release(), arc_off.release(), arc.release();
+	len.release(), base.release(), pk.release(), raw.release(), arc_off.release(), arc.release();
 	if (cur >= 0) cudaSetDevice(cur);
 }
 
@@ -178,22 +177,17 @@ static int upload_graph(const gwf_graph_t *g, GraphDev *G)
 	std::vector<uint32_t> off(nv + 1, 0);
 	for (uint32_t e = 0; e < g->n_arc; ++e) off[(uint32_t)(g->arc[e].a >> 32) + 1]++;
 	for (uint32_t v = 0; v < nv; ++v) off[v + 1] += off[v];
-	std::vector<uint4> vtx(nv ? nv : 1);
-	for (uint32_t v = 0; v < nv; ++v)
-		vtx[v] = make_uint4((uint32_t)base[v], (uint32_t)(base[v] >> 32), len[v], off[v]);
 	std::vector<uint2> arc(g->n_arc ? g->n_arc : 1);
 	for (uint32_t e = 0; e < g->n_arc; ++e) arc[e] = make_uint2((uint32_t)g->arc[e].a, (uint32_t)g->arc[e].o);
 	G->n_vtx = nv, G->n_arc = g->n_arc, G->pure = pure, G->total_len = tot;
 	G->dens_milli = (int32_t)std::max<uint64_t>(1, (uint64_t)nv * 1000 / std::max<uint64_t>(1, tot));
 	int rc;
-	if ((rc = G->vtx.ensure(sizeof(uint4) * vtx.size()))) return rc;
 	if ((rc = G->len.ensure(sizeof(uint32_t) * std::max<size_t>(nv, 1)))) return rc;
 	if ((rc = G->base.ensure(sizeof(uint64_t) * std::max<size_t>(nv, 1)))) return rc;
 	if ((rc = G->pk.ensure(sizeof(uint64_t) * nw))) return rc;
 	if ((rc = G->raw.ensure(raw.size()))) return rc;
 	if ((rc = G->arc_off.ensure(sizeof(uint32_t) * (nv + 1)))) return rc;
 	if ((rc = G->arc.ensure(sizeof(uint2) * arc.size()))) return rc;
-	CK(cudaMemcpy(G->vtx.p, vtx.data(), sizeof(uint4) * vtx.size(), cudaMemcpyHostToDevice));
 	CK(cudaMemcpy(G->len.p, len.data(), sizeof(uint32_t) * nv, cudaMemcpyHostToDevice));
 	CK(cudaMemcpy(G->base.p, base.data(), sizeof(uint64_t) * nv, cudaMemcpyHostToDevice));
 	CK(cudaMemcpy(G->pk.p, pk.data(), sizeof(uint64_t) * nw, cudaMemcpyHostToDevice));
@@ -293,6 +287,11 @@ Engine *gwf_engine(int dev)
 		return nullptr;
 	}
 	cudaDeviceGetAttribute(&E->sm_count, cudaDevAttrMultiProcessorCount, dev);
+	{
+		size_t fr = 0, tot = 0;
+		cudaMemGetInfo(&fr, &tot);
+		E->mem_budget = (int64_t)(fr / 2);
+	}
 	int occ = 0;
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_align_persistent, 256, 0);
 	E->persistent_ctas_per_sm = occ > 0 ? occ : 1;
@@ -329,13 +328,18 @@ int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64
 	int64_t words = 0;
 	for (int32_t i = 0; i < n; ++i) B.h_pk_off[(size_t)i] = words, words += (ql[i] + 31) / 32 + 2;
 	B.pk_words = words;
-	// persistent queue: longest reads first (LPT scheduling on a cost ~ length estimate)
-	B.h_order.resize((size_t)n);
-	std::iota(B.h_order.begin(), B.h_order.end(), 0);
-	std::stable_sort(B.h_order.begin(), B.h_order.end(),
-	                 [&](int32_t x, int32_t y) { return ql[x] > ql[y]; });
+	// persistent queue: longest reads first (LPT scheduling on a cost ~ length estimate), as a
+	// counting sort over 64-base length buckets
 	B.max_ql = 0;
 	for (int32_t i = 0; i < n; ++i) B.max_ql = std::max(B.max_ql, ql[i]);
+	{
+		const int32_t nb = (B.max_ql >> 6) + 1;
+		std::vector<int32_t> cnt((size_t)nb + 1, 0);
+		for (int32_t i = 0; i < n; ++i) cnt[(size_t)(nb - 1 - (ql[i] >> 6)) + 1]++;
+		for (int32_t b = 0; b < nb; ++b) cnt[(size_t)b + 1] += cnt[(size_t)b];
+		B.h_order.resize((size_t)n);
+		for (int32_t i = 0; i < n; ++i) B.h_order[(size_t)cnt[(size_t)(nb - 1 - (ql[i] >> 6))]++] = i;
+	}
 	const size_t nraw = (size_t)(hi - lo) + 16;
 	int rc;
 	if ((rc = B.raw.ensure(nraw)) || (rc = B.raw_off.ensure(8 * (size_t)n + 8)) ||
@@ -402,10 +406,9 @@ static int launch_persistent(Engine &E, KParams p, const int32_t *d_order, int32
 	int64_t warps = (int64_t)E.sm_count * ctas_per_sm * kWarpsPerCta;
 	const int64_t need_warps = (n_order + 0LL);
 	if (warps > need_warps) warps = std::max<int64_t>(kWarpsPerCta, ((need_warps + kWarpsPerCta - 1) / kWarpsPerCta) * kWarpsPerCta);
-	// keep arenas within a budget of the free device memory
-	size_t fr = 0, tot = 0;
-	cudaMemGetInfo(&fr, &tot);
-	const int64_t budget = (int64_t)(fr * 6 / 10) + (int64_t)E.ws.cap;
+	// keep arenas within a budget of the device memory (free memory sampled when the engine
+	// was created, plus what the arena already holds)
+	const int64_t budget = E.mem_budget + (int64_t)E.ws.cap;
 	while (warps > kWarpsPerCta && warps * slot > budget) warps -= kWarpsPerCta;
 	if (warps * slot > budget) {
 		gwf_set_errorf("arena of %lld bytes per warp does not fit the device", (long long)slot);
@@ -433,9 +436,7 @@ static int launch_persistent(Engine &E, KParams p, const int32_t *d_order, int32
 // arenas of all reads do not fit).
 static int launch_plain(Engine &E, KParams p, Batch &B, int *launches)
 {
-	size_t fr = 0, tot = 0;
-	cudaMemGetInfo(&fr, &tot);
-	const int64_t budget = (int64_t)(fr * 6 / 10) + (int64_t)E.ws.cap;
+	const int64_t budget = E.mem_budget + (int64_t)E.ws.cap;
 	int32_t start = 0;
 	std::vector<int64_t> offs;
 	while (start < B.n) {

@@ -27,7 +27,7 @@ struct GraphDev { // device-resident copy of one gwf_graph_t
 	uint32_t n_vtx = 0, n_arc = 0;
 	int32_t pure = 0, dens_milli = 1;
 	uint64_t total_len = 0;
-	DBuf vtx, len, base, pk, raw, arc_off, arc;
+	DBuf len, base, pk, raw, arc_off, arc;
 	gwfb::DevGraph view() const;
 	~GraphDev();
 };
@@ -36,6 +36,7 @@ struct Engine { // per-device launch state: stream, events, warp arenas
 	int device = 0;
 	int sm_count = 0;
 	int persistent_ctas_per_sm = 1;
+	int64_t mem_budget = 0; // device bytes the arenas may take
 	cudaStream_t stream = nullptr;
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 	DBuf pk_off, order, head, retry_list, retry_n, ws, slot_off, w_out;

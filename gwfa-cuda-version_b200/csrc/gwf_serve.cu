@@ -175,6 +175,7 @@ extern "C" gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t 
 		cudaDeviceGetAttribute(&E->sm_count, cudaDevAttrMultiProcessorCount, dev);
 		Engine *ref = gwf_engine(dev);
 		E->persistent_ctas_per_sm = ref ? ref->persistent_ctas_per_sm : 1;
+		E->mem_budget = ref ? ref->mem_budget / n_lanes : ((int64_t)1 << 30);
 		S->engines.push_back(E);
 	}
 	if (S->engines.empty()) {
