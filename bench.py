@@ -191,6 +191,118 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def make_requests(w, rng, max_reads=256):
+    """Split the workload's reads into consecutive requests of U{1..max_reads} reads."""
+    n = len(w["lens"])
+    reqs, i = [], 0
+    while i < n:
+        m = int(rng.integers(1, max_reads + 1))
+        idx = np.arange(i, min(n, i + m))
+        reqs.append(((w["cat"], np.ascontiguousarray(w["offs"][idx]), np.ascontiguousarray(w["lens"][idx])),
+                     np.ascontiguousarray(w["v0"][idx])))
+        i += m
+    return reqs
+
+
+def serve_stream(srv, reqs, rate_rps, rng):
+    """Submits requests at seeded Poisson arrival times (rate in requests/s; 0 = all at once) and
+    waits for all. Returns per-request latency (done - submit) and the span from the first
+    submit to the last completion."""
+    gaps = rng.exponential(1.0 / rate_rps, len(reqs)) if rate_rps > 0 else np.zeros(len(reqs))
+    ids = []
+    t_next = time.perf_counter()
+    for (reads, v0), gap in zip(reqs, gaps):
+        t_next += gap
+        d = t_next - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        ids.append(srv.submit(reads, v0))
+    lat, first, last = [], None, None
+    for rid, k in ids:
+        _, st = srv.wait(rid, k, timeout_s=600)
+        if not (st == 0).all():
+            raise RuntimeError("serving request %d: read status %s" % (rid, np.unique(st)))
+        ts, _, td = srv.times(rid)
+        lat.append(td - ts)
+        first = ts if first is None else min(first, ts)
+        last = td if last is None else max(last, td)
+    return np.array(lat), last - first
+
+
+def fifo_replay(arrivals, service):
+    """Latency of a single FIFO server (one launch per request, one after another)."""
+    lat, free = [], 0.0
+    for a, s in zip(arrivals, service):
+        start = max(a, free)
+        free = start + s
+        lat.append(free - a)
+    return np.array(lat)
+
+
+def run_serving(args):
+    """Serving on the 5 Mbp graph (resident): requests of U{1..256} reads, ql U[500, 20000],
+    error U[1%, 10%], seeded Poisson arrivals at 50/70/90% of the measured peak, admission by a
+    fixed arena budget. Plain baseline: one plain launch per request, served FIFO."""
+    G = pkg()
+    w = G.load_workload("config5", n=args.serve_reads)
+    g = w["graph"]
+    g.index()
+    budget = int(args.serve_budget_gib * (1 << 30))
+    srv = G.Server(g, arena_budget_bytes=budget)
+    rng = np.random.default_rng(55)
+    reqs = make_requests(w, rng)
+    nreads = [len(r[1]) for r in reqs]
+    mean_req = float(np.mean(nreads))
+    # warm-up, then peak: every request submitted at once
+    serve_stream(srv, reqs[:4], 0, rng)
+    with ClockSampler(0) as clk:
+        _, span = serve_stream(srv, reqs, 0, rng)
+        peak = sum(nreads) / span
+        print("serving peak %.1f reads/s over %.1f s" % (peak, span), file=sys.stderr, flush=True)
+        levels = {}
+        for frac in (0.5, 0.7, 0.9):
+            rate = frac * peak / mean_req
+            lat, span = serve_stream(srv, reqs, rate, np.random.default_rng(int(frac * 100)))
+            key = "%d%%" % int(frac * 100)
+            levels[key] = {"offered_reads_per_s": frac * peak, "reads_per_s": sum(nreads) / span,
+                           "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                           "requests": len(reqs)}
+            print("serving at %s: %s" % (key, levels[key]), file=sys.stderr, flush=True)
+    stats = srv.stats()
+    srv.close()
+    # plain one-launch-per-request: measured launch times on a sample, FIFO replay per level
+    sample = reqs[:args.plain_sample]
+    svc = []
+    for reads, v0 in sample:
+        t0 = time.perf_counter()
+        g.ed_batch(reads, v0, mode=G.MODE_PLAIN)
+        svc.append(time.perf_counter() - t0)
+        print("plain request of %d reads: %.2f s" % (len(v0), svc[-1]), file=sys.stderr, flush=True)
+    plain_cap = sum(nreads[:len(sample)]) / sum(svc)
+    service = [svc[i % len(svc)] for i in range(len(reqs))]
+    plain = {"reads_per_s_capacity": plain_cap, "sample_requests": len(sample)}
+    for frac in (0.5, 0.7, 0.9):
+        rate = frac * peak / mean_req
+        arr = np.cumsum(np.random.default_rng(int(frac * 100)).exponential(1.0 / rate, len(reqs)))
+        lat = fifo_replay(arr, service)
+        plain["%d%%" % int(frac * 100)] = {"p50_s": float(np.percentile(lat, 50)),
+                                           "p99_s": float(np.percentile(lat, 99))}
+    line = {
+        "metric": "serving p50/p99 request latency and reads/s at 50/70/90% of peak offered load",
+        "value": levels["70%"]["p99_s"], "unit": "s (p99 at 70% of peak)", "n_gpus": 1,
+        "higher_is_better": False, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "config5: 5 Mbp graph resident; requests of U{1..256} reads, ql U[500,20000], "
+                               "error U[1%,10%]; seeded Poisson arrivals", "reads": int(sum(nreads)),
+                   "requests": len(reqs), "arena_budget_gib": args.serve_budget_gib},
+        "peak_reads_per_s": peak, "levels": levels, "server": stats,
+        "plain_one_launch_per_request": plain,
+        "plain_note": "plain capacity from measured per-request launches; latency by FIFO replay of the same "
+                      "arrivals (the sample's launch times, cycled)",
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -203,8 +315,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-step-seconds", type=float, default=8.0)
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="persistent grid; 0 = occupancy limit")
+    ap.add_argument("--serving", action="store_true", help="serving benchmark (config5) instead")
+    ap.add_argument("--serve-reads", type=int, default=12000)
+    ap.add_argument("--serve-budget-gib", type=float, default=64.0)
+    ap.add_argument("--plain-sample", type=int, default=6)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.serving:
+        run_serving(args)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -94,10 +94,12 @@ __host__ __device__ inline Caps caps_for(int32_t ql, int32_t level, int32_t dens
 	c.tb = c.a;
 	c.ta = pow2ceil_i(c.a / 2 > 64 ? c.a / 2 : 64);
 	c.iv = c.a / 2 + 64;
-	// expected arrival keys ~ density * 0.1 * ql^2, at most the reference's 32 * ql
+	// expected arrival keys ~ density * 0.1 * ql^2 (the reference caps its set at 32 * ql keys;
+	// reads of 20 kbp on a graph with a variant every 50 bp reach ~90 * ql, so cap at 64 * ql and
+	// let the retry classes take the rest)
 	int64_t est = (int64_t)dens_milli * q * q / 10000;
 	if (est < 256) est = 256;
-	if (est > 32 * q) est = 32 * q;
+	if (est > 64 * q) est = 64 * q;
 	est = est * 2 * mult;
 	if (est > (1 << 26)) est = 1 << 26;
 	c.h = pow2ceil_i((int32_t)est);
@@ -185,22 +187,17 @@ __device__ __forceinline__ uint64_t warp_incl_max(uint64_t x)
 	return x;
 }
 
-// 32 consecutive bases (2 bits each) starting at base position pos; words little-endian.
-__device__ __forceinline__ uint64_t window2(const uint64_t *__restrict__ pk, int64_t pos)
-{
-	int64_t w = pos >> 5;
-	int sh = (int)(pos & 31) * 2;
-	uint64_t lo = __ldg(pk + w), hi = __ldg(pk + w + 1);
-	return sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
-}
 // 8 consecutive bytes starting at p + pos, read as two aligned words (the buffer behind p starts
 // 8-byte aligned and carries 16 bytes of padding).
+// RO: the bytes are read-only for the kernel's lifetime (graph), so the non-coherent path is
+// allowed; query bytes may be written earlier in the same kernel (serving) and use plain loads.
+template <bool RO>
 __device__ __forceinline__ uint64_t window8(const uint8_t *p, int64_t pos)
 {
 	const uintptr_t a = (uintptr_t)(p + pos);
 	const uint64_t *w = (const uint64_t *)(a & ~(uintptr_t)7);
 	const int sh = (int)(a & 7) * 8;
-	const uint64_t lo = __ldg(w), hi = __ldg(w + 1);
+	const uint64_t lo = RO ? __ldg(w) : w[0], hi = RO ? __ldg(w + 1) : w[1];
 	return sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
 }
 
@@ -214,12 +211,12 @@ struct ReadCtx {
 
 // 32 bases starting at base position pos of a 2-bit packed sequence, as (lo, hi) 16-base
 // halves: three aligned 32-bit loads and two funnel shifts (the arrays carry padding words).
-__device__ __forceinline__ void window32(const uint32_t *__restrict__ pk, int64_t pos, uint32_t &lo,
-                                        uint32_t &hi)
+template <bool RO>
+__device__ __forceinline__ void window32(const uint32_t *pk, int64_t pos, uint32_t &lo, uint32_t &hi)
 {
 	const uint32_t *w = pk + (pos >> 4);
 	const uint32_t sh = (uint32_t)(pos & 15) * 2;
-	const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+	const uint32_t w0 = RO ? __ldg(w) : w[0], w1 = RO ? __ldg(w + 1) : w[1], w2 = RO ? __ldg(w + 2) : w[2];
 	lo = __funnelshift_r(w0, w1, sh);
 	hi = __funnelshift_r(w1, w2, sh);
 }
@@ -237,8 +234,8 @@ __device__ __forceinline__ int32_t ext(const DevGraph &g, const ReadCtx &rc, uin
 		const uint32_t *gp = (const uint32_t *)g.pk, *qp = (const uint32_t *)rc.qpk;
 		for (int guard = 0; k < m && guard < (1 << 26); ++guard) {
 			uint32_t glo, ghi, qlo, qhi;
-			window32(gp, gb + k + 1, glo, ghi);
-			window32(qp, (int64_t)d + k + 1, qlo, qhi);
+			window32<true>(gp, gb + k + 1, glo, ghi);
+			window32<false>(qp, (int64_t)d + k + 1, qlo, qhi);
 			uint32_t xlo = glo ^ qlo, xhi = ghi ^ qhi;
 			const int32_t rem = m - k; // bases left to compare, >= 1
 			if (rem < 16) xlo |= ~0u << (2 * rem), xhi = ~0u;
@@ -253,7 +250,7 @@ __device__ __forceinline__ int32_t ext(const DevGraph &g, const ReadCtx &rc, uin
 	} else {
 		for (int guard = 0; k < m && guard < (1 << 28); ++guard) {
 			const int32_t rem = m - k;
-			uint64_t x = window8(g.raw, gb + k + 1) ^ window8(rc.qraw, (int64_t)d + k + 1);
+			uint64_t x = window8<true>(g.raw, gb + k + 1) ^ window8<false>(rc.qraw, (int64_t)d + k + 1);
 			if (rem < 8) x |= ~0ULL << (8 * rem);
 			if (x == 0) {
 				k += 8;
@@ -273,10 +270,10 @@ __device__ __forceinline__ bool base_eq(const DevGraph &g, const ReadCtx &rc, ui
 	const int64_t gp = (int64_t)__ldg(g.base + w) + o;
 	if (rc.packed) {
 		uint64_t a = __ldg(g.pk + (gp >> 5)) >> ((gp & 31) * 2);
-		uint64_t b = __ldg(rc.qpk + (i >> 5)) >> ((i & 31) * 2);
+		uint64_t b = rc.qpk[i >> 5] >> ((i & 31) * 2);
 		return ((a ^ b) & 3) == 0;
 	}
-	return __ldg(g.raw + gp) == __ldg(rc.qraw + i);
+	return __ldg(g.raw + gp) == rc.qraw[i];
 }
 
 // Arrival set (static_set64_put, gwf-ed.cu:1020-1062): open addressing, linear probing,

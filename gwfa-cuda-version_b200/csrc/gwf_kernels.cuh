@@ -26,6 +26,55 @@ struct KParams {
 	int64_t *w_out;         // optional per-read sum of wavefront sizes
 };
 
+// ---- serving: one resident kernel, warps pull single reads from a device queue
+//
+// Each queued read owns an arena (allocated by the host from a fixed budget) laid out as
+//   [0, 256)              SrvHdr
+//   [256, 256 + pkb)      2-bit packed read, written by the warp
+//   [.., + rawb)          raw read bytes (+16 padding), copied in by the host before publication
+//   [srv_qbytes(ql), ..)  wavefront workspace for caps_for(ql, level)
+struct SrvEntry {         // queue entry, 48 bytes
+	uint32_t seq;         // queue position + 1 (checks that the entry is the one claimed)
+	int32_t tag;          // host slot of the read
+	int64_t arena_off;    // byte offset of the read's arena in the pool
+	int64_t arena_bytes;
+	int32_t ql, v0, v1, level;
+	int32_t pad[2];
+};
+struct SrvDone {          // completion record in host-mapped memory
+	int32_t tag, dist, status, gen; // gen = pass over the ring + 1, written last
+};
+struct SrvHdr {
+	int64_t zero;
+	int32_t ql, v0, dist, status;
+	uint8_t pure, pad[7];
+};
+struct SrvParams {
+	DevGraph g;
+	const SrvEntry *q;                 // device ring, qmask + 1 entries
+	const unsigned long long *q_tail;  // published by the host (device memory)
+	unsigned long long *q_head;        // next position to claim
+	const int32_t *stop;               // host sets 1 to end the kernel
+	int32_t *busy;                     // warps holding a read
+	unsigned long long *cq_tail;       // next completion position
+	SrvDone *cq;                       // host-mapped ring, cmask + 1 records
+	int32_t *err;                      // host-mapped error bits (SRV_ERR_*)
+	uint8_t *arena;                    // arena pool
+	uint32_t qmask, cmask;
+	int32_t cq_shift;                  // log2(cmask + 1)
+	int32_t dens_milli, flags;
+	int64_t idle_ns;                   // an idle warp leaves after this when no warp is busy
+	int64_t max_idle_ns;               // and after this in any case
+};
+constexpr int32_t SRV_ERR_SEQ = 1;     // a claimed entry did not carry its position
+
+__host__ __device__ inline int64_t srv_al256(int64_t x) { return (x + 255) & ~255LL; }
+__host__ __device__ inline int64_t srv_pk_bytes(int32_t ql) { return srv_al256(8LL * ((ql + 31) / 32 + 2)); }
+__host__ __device__ inline int64_t srv_qbytes(int32_t ql)
+{
+	return 256 + srv_pk_bytes(ql) + srv_al256((int64_t)ql + 16);
+}
+
 #ifndef GWF_KERNELS_DECL_ONLY
 // Aligns read r with one warp. All control flow is warp-uniform.
 __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *wsb, const Caps &c)
@@ -501,19 +550,151 @@ __global__ void __launch_bounds__(256, 3) k_align_plain(const __grid_constant__ 
 	align_read(p, r, p.ws + p.slot_off[gw], c);
 }
 
-// Persistent form: each warp owns one arena and pulls reads from the cost-ordered queue.
+// Persistent form: each warp owns one arena (sized for ql_cap) and pulls reads from the
+// cost-ordered queue; each read uses the capacities of its own length, so a short read clears
+// and touches only the arena it needs.
 __global__ void __launch_bounds__(256, 3) k_align_persistent(const __grid_constant__ KParams p)
 {
 	const int lane = threadIdx.x & 31;
 	const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-	const Caps c = caps_for(p.ql_cap, p.level, p.dens_milli);
 	uint8_t *wsb = p.ws + gw * p.slot_bytes;
 	for (int32_t guard = 0; guard < p.n_order + 1; ++guard) {
 		int32_t qi = 0;
 		if (lane == 0) qi = atomicAdd(p.head, 1);
 		qi = __shfl_sync(FULL, qi, 0);
 		if (qi >= p.n_order) break;
-		align_read(p, p.order[qi], wsb, c);
+		const int32_t r = p.order[qi];
+		const int32_t ql = p.r.ql[r];
+		align_read(p, r, wsb, caps_for(ql < p.ql_cap ? ql : p.ql_cap, p.level, p.dens_milli));
+	}
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns()
+{
+	uint64_t t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p)
+{
+	unsigned long long v;
+	asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+	return v;
+}
+__device__ __forceinline__ int32_t ld_acquire_s32(const int32_t *p)
+{
+	int32_t v;
+	asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+	return v;
+}
+
+// Serving form. A warp claims the next published queue position (bounded, backed-off polling of
+// device memory), packs the read that the host copied into its arena, aligns it at the entry's
+// capacity class, and writes a completion record into host-mapped memory (an arena overflow
+// comes back as GWF_E_CAPACITY; the host re-queues the read in a larger arena). Idle warps leave
+// after idle_ns once no warp holds a read, and after max_idle_ns in any case; the host relaunches
+// the kernel when work is queued and it has ended.
+__global__ void __launch_bounds__(256, 3) k_serve(const __grid_constant__ SrvParams p)
+{
+	const int lane = threadIdx.x & 31;
+	for (int64_t guard = 0; guard < (1LL << 40); ++guard) {
+		long long h = -1;
+		if (lane == 0) {
+			const uint64_t t0 = globaltimer_ns();
+			uint32_t ns = 128;
+			for (int64_t spin = 0; spin < (1LL << 32); ++spin) {
+				if (ld_acquire_s32(p.stop)) break;
+				const unsigned long long tail = ld_acquire_u64(p.q_tail);
+				const unsigned long long head = *(volatile const unsigned long long *)p.q_head;
+				if (head < tail) {
+					if (atomicCAS(p.q_head, head, head + 1) == head) {
+						h = (long long)head;
+						break;
+					}
+					continue;
+				}
+				const int64_t idle = (int64_t)(globaltimer_ns() - t0);
+				if (idle > p.max_idle_ns) break;
+				if (idle > p.idle_ns && *(volatile const int32_t *)p.busy == 0) break;
+				__nanosleep(ns);
+				if (ns < 16384) ns *= 2;
+			}
+			if (h >= 0) atomicAdd(p.busy, 1);
+		}
+		h = __shfl_sync(FULL, h, 0);
+		if (h < 0) break;
+		__syncwarp();
+		asm volatile("fence.acq_rel.gpu;" ::: "memory");
+		const SrvEntry *ep = p.q + (h & p.qmask);
+		const uint32_t seq = __ldcg((const unsigned int *)&ep->seq);
+		if (seq != (uint32_t)(h + 1)) { // cannot happen while the host keeps its ring bounds
+			if (lane == 0) atomicOr(p.err, SRV_ERR_SEQ), atomicSub(p.busy, 1);
+			break;
+		}
+		const int32_t tag = __ldcg(&ep->tag), ql = __ldcg(&ep->ql), v0 = __ldcg(&ep->v0);
+		const int32_t v1 = __ldcg(&ep->v1), level = __ldcg(&ep->level);
+		const long long aoff = __ldcg((const long long *)&ep->arena_off);
+		const long long abytes = __ldcg((const long long *)&ep->arena_bytes);
+		uint8_t *ab = p.arena + aoff;
+		SrvHdr *hdr = (SrvHdr *)ab;
+		uint64_t *pk = (uint64_t *)(ab + 256);
+		const uint8_t *raw = ab + 256 + srv_pk_bytes(ql);
+		// pack as k_pack_reads does; the raw bytes came by DMA, so they are read from L2
+		const int32_t L = ql > 0 ? ql : 0;
+		const int32_t nw = (L + 31) / 32 + 2;
+		bool ok = true;
+		for (int32_t w = lane; w < nw; w += 32) {
+			uint64_t word = 0;
+			for (int32_t t = 0; t < 32; ++t) {
+				const int32_t i = w * 32 + t;
+				if (i < L) {
+					const uint8_t ch = (uint8_t)__ldcg((const unsigned char *)raw + i);
+					ok &= (ch == 'A' || ch == 'C' || ch == 'G' || ch == 'T');
+					word |= (uint64_t)((ch >> 1) & 3) << (2 * t);
+				}
+			}
+			pk[w] = word;
+		}
+		ok = __all_sync(FULL, ok);
+		if (lane == 0) {
+			hdr->zero = 0, hdr->ql = ql, hdr->v0 = v0, hdr->pure = ok ? 1 : 0;
+			hdr->dist = -1, hdr->status = ST_CAPACITY;
+		}
+		__syncwarp();
+		int32_t dist = -1, st = ST_CAPACITY;
+		const int64_t qb = srv_qbytes(ql);
+		const Caps c = caps_for(ql, level, p.dens_milli);
+		if (qb + ws_layout(c).total <= abytes) { // the host sized it so; else report capacity
+			KParams lp;
+			memset(&lp, 0, sizeof lp);
+			lp.g = p.g;
+			lp.r.pk = pk;
+			lp.r.pk_off = &hdr->zero;
+			lp.r.raw = raw;
+			lp.r.raw_off = &hdr->zero;
+			lp.r.ql = &hdr->ql;
+			lp.r.v0 = &hdr->v0;
+			lp.r.pure = &hdr->pure;
+			lp.r.v1 = v1;
+			lp.r.n = 1;
+			lp.dens_milli = p.dens_milli;
+			lp.flags = p.flags;
+			lp.dist = &hdr->dist;
+			lp.status = &hdr->status;
+			align_read(lp, 0, ab + qb, c);
+			__syncwarp();
+			dist = *(volatile int32_t *)&hdr->dist;
+			st = *(volatile int32_t *)&hdr->status;
+		}
+		if (lane == 0) {
+			const unsigned long long pos = atomicAdd(p.cq_tail, 1ULL);
+			volatile SrvDone *d = p.cq + (pos & p.cmask);
+			d->tag = tag, d->dist = dist, d->status = st;
+			__threadfence_system();
+			d->gen = (int32_t)((pos >> p.cq_shift) + 1);
+			atomicSub(p.busy, 1);
+		}
+		__syncwarp();
 	}
 }
 

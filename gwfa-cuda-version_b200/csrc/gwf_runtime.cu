@@ -545,6 +545,22 @@ cudaError_t gwf_launch_persistent(const KParams &p, int ctas, int threads, cudaS
 	return cudaGetLastError();
 }
 
+cudaError_t gwf_launch_serve(const SrvParams &p, int ctas, int threads, cudaStream_t s)
+{
+	k_serve<<<ctas, threads, 0, s>>>(p);
+	return cudaGetLastError();
+}
+
+int gwf_serve_ctas_per_sm()
+{
+	int occ = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_serve, 256, 0) != cudaSuccess) {
+		cudaGetLastError();
+		return 1;
+	}
+	return occ > 0 ? occ : 1;
+}
+
 // ------------------------------------------------------------------ public batch entry points
 static std::mutex g_batch_mu; // batch calls are serialised (one engine per device)
 static std::unordered_map<int, Batch *> g_scratch_batches;

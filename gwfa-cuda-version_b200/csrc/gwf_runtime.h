@@ -63,5 +63,8 @@ int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t
 int gwf_batch_fetch(Engine &E, Batch &B, int32_t *dist, int32_t *status);
 namespace gwfb {
 struct KParams;
+struct SrvParams;
 }
 cudaError_t gwf_launch_persistent(const gwfb::KParams &p, int ctas, int threads, cudaStream_t s);
+cudaError_t gwf_launch_serve(const gwfb::SrvParams &p, int ctas, int threads, cudaStream_t s);
+int gwf_serve_ctas_per_sm();

@@ -1,27 +1,42 @@
 // gwf_serve.cu — continuous-batching request loop on a device-resident graph.
 //
-// Requests (1..n reads each) queue in FIFO order. K lanes, each a host thread with its own CUDA
-// stream and warp arenas, take as many queued requests as their share of the arena budget
-// admits and run them through the persistent kernel. While one lane's launch is on the GPU the
-// others admit newly arrived requests, so work from different requests overlaps on the device.
-// A request is complete when every read has a distance or a per-read error status; its submit,
-// admit and completion times are kept for latency percentiles.
+// One resident kernel (k_serve) runs on the device; its warps pull single reads from a queue in
+// device memory. A host pump thread does everything else:
+//   * admission: reads of queued requests are admitted in FIFO order while a slot is free and the
+//     arena pool (a fixed device-memory budget) has room for the read's wavefront arena, sized for
+//     its own length; the read's bases are copied into its arena and its queue entry published;
+//   * completion: the kernel writes one record per read into host-mapped memory; the pump frees
+//     the arena and the slot, and completes a request when its last read is done;
+//   * retry: a read that overflows its arena comes back with GWF_E_CAPACITY and is queued again
+//     in a 4x larger arena (up to three times), ahead of new reads;
+//   * liveness: idle warps leave after a few milliseconds once no warp is busy; the pump
+//     relaunches the kernel when positions are queued and it has ended.
+// Reads that arrive while others are on the device therefore start as soon as a warp and arena
+// memory are free, and results do not depend on what else is in flight.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <thread>
 #include <unordered_map>
 #include <vector>
 
 #include "../../include/gwfa.h"
+#define GWF_KERNELS_DECL_ONLY
+#include "gwf_kernels.cuh"
 #include "gwf_runtime.h"
 #include "gwfa_internal.h"
+
+using gwfb::SrvDone;
+using gwfb::SrvEntry;
 
 namespace {
 
@@ -30,15 +45,78 @@ double now_s()
 	return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+constexpr int kMaxLevel = 3;         // arena classes 1x, 4x, 16x, 64x, as the batch path
+constexpr int64_t kIdleNs = 5000000; // 5 ms
+constexpr int64_t kMaxIdleNs = 30LL * 1000000000LL;
+
+// Best-fit allocator over [0, cap) in 256-byte units, with coalescing.
+class Pool {
+public:
+	void init(int64_t cap)
+	{
+		cap_ = cap & ~255LL;
+		by_off_.clear(), by_size_.clear();
+		if (cap_ > 0) insert(0, cap_);
+		used_ = 0;
+	}
+	int64_t alloc(int64_t bytes)
+	{
+		bytes = (bytes + 255) & ~255LL;
+		auto it = by_size_.lower_bound({bytes, -1});
+		if (it == by_size_.end()) return -1;
+		const int64_t off = it->second, sz = it->first;
+		erase(off, sz);
+		if (sz > bytes) insert(off + bytes, sz - bytes);
+		used_ += bytes;
+		return off;
+	}
+	void release(int64_t off, int64_t bytes)
+	{
+		bytes = (bytes + 255) & ~255LL;
+		used_ -= bytes;
+		auto nx = by_off_.lower_bound(off);
+		if (nx != by_off_.end() && nx->first == off + bytes) {
+			const int64_t s = nx->second;
+			erase(nx->first, s);
+			bytes += s;
+		}
+		auto pv = by_off_.lower_bound(off);
+		if (pv != by_off_.begin()) {
+			--pv;
+			if (pv->first + pv->second == off) {
+				const int64_t o = pv->first, s = pv->second;
+				erase(o, s);
+				off = o, bytes += s;
+			}
+		}
+		insert(off, bytes);
+	}
+	int64_t used() const { return used_; }
+	int64_t cap() const { return cap_; }
+
+private:
+	void insert(int64_t off, int64_t sz) { by_off_[off] = sz, by_size_.insert({sz, off}); }
+	void erase(int64_t off, int64_t sz) { by_off_.erase(off), by_size_.erase({sz, off}); }
+	std::map<int64_t, int64_t> by_off_;
+	std::set<std::pair<int64_t, int64_t>> by_size_;
+	int64_t cap_ = 0, used_ = 0;
+};
+
 struct Request {
-	int64_t id;
-	int32_t n, v1;
+	int64_t id = 0;
+	int32_t n = 0, v1 = -1;
 	std::vector<char> seqs;
 	std::vector<int64_t> offs;
 	std::vector<int32_t> ql, v0, dist, status;
+	int32_t next_read = 0, n_done = 0;
 	double t_submit = 0, t_admit = 0, t_done = 0;
 	bool done = false;
-	int32_t error = 0;
+};
+
+struct Slot {
+	std::shared_ptr<Request> r;
+	int32_t read = 0, level = 0;
+	int64_t off = -1, bytes = 0;
 };
 
 } // namespace
@@ -46,104 +124,312 @@ struct Request {
 struct gwf_srv_s {
 	const gwf_graph_t *g = nullptr;
 	GraphDev *G = nullptr;
-	int device = 0;
+	int device = 0, sm_count = 0, ctas = 0;
 	int32_t flags = 0;
 	int64_t budget = 0;
-	int32_t max_reads = 0;
-	std::mutex mu;
-	std::condition_variable cv_work, cv_done;
+	uint32_t qcap = 0, ccap = 0;
+	int cq_shift = 0;
+	cudaStream_t kstream = nullptr, fstream = nullptr;
+	cudaEvent_t kdone = nullptr;
+	bool kernel_running = false;
+	// device memory: arena pool, queue ring, control words
+	DBuf pool_mem, q_mem, ctl;
+	// host memory: completion ring + error word (mapped), queue mirror + control values (pinned)
+	void *mapped = nullptr, *pinned = nullptr;
+	volatile SrvDone *cq = nullptr;
+	volatile int32_t *err = nullptr;
+	SrvDone *cq_dev = nullptr;
+	int32_t *err_dev = nullptr;
+	SrvEntry *h_q = nullptr;
+	unsigned long long *h_tail = nullptr;
+	int32_t *h_stop = nullptr;
+	Pool pool;
+	std::vector<Slot> slots;
+	std::vector<int32_t> free_slots;
+	std::deque<int32_t> retry;
 	std::deque<std::shared_ptr<Request>> pending;
 	std::unordered_map<int64_t, std::shared_ptr<Request>> all;
-	int64_t next_id = 0;
+	uint64_t q_pos = 0, cq_pos = 0;
+	int64_t in_flight = 0;
+	std::mutex mu;
+	std::condition_variable cv_work, cv_done;
 	bool stop = false;
-	std::vector<std::thread> lanes;
-	std::vector<Engine *> engines;
+	int fatal = 0;
+	int64_t next_id = 0;
+	std::thread pump;
+	int64_t launches = 0, retries = 0;
 };
 
-static void lane_main(gwf_srv_s *S, int lane_id)
+namespace {
+
+unsigned long long *q_tail_dev(gwf_srv_s *S) { return (unsigned long long *)S->ctl.p; }
+unsigned long long *q_head_dev(gwf_srv_s *S) { return (unsigned long long *)S->ctl.p + 1; }
+unsigned long long *cq_tail_dev(gwf_srv_s *S) { return (unsigned long long *)S->ctl.p + 2; }
+int32_t *stop_dev(gwf_srv_s *S) { return (int32_t *)((unsigned long long *)S->ctl.p + 3); }
+int32_t *busy_dev(gwf_srv_s *S) { return stop_dev(S) + 1; }
+
+int64_t arena_bytes(const gwf_srv_s *S, int32_t ql, int32_t level)
 {
-	cudaSetDevice(S->device);
-	Engine *E = S->engines[(size_t)lane_id];
-	Batch B;
-	const int64_t lane_budget = S->budget / (int64_t)S->engines.size();
-	for (;;) {
-		std::vector<std::shared_ptr<Request>> take;
-		{
-			std::unique_lock<std::mutex> lk(S->mu);
-			S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty(); });
-			if (S->stop && S->pending.empty()) break;
-			int32_t reads = 0, qmax = 0;
-			while (!S->pending.empty()) {
-				auto &r = S->pending.front();
-				int32_t rq = 0;
-				for (int32_t x : r->ql) rq = std::max(rq, x);
-				const int32_t nq = std::max(qmax, rq);
-				// arena estimate: one warp per read, arenas sized for the longest read
-				const int64_t need = (int64_t)(reads + r->n) *
-				                     gwfb::ws_layout(gwfb::caps_for(nq, 0, S->G->dens_milli)).total;
-				if (!take.empty() && (need > lane_budget || reads + r->n > S->max_reads)) break;
-				reads += r->n, qmax = nq;
-				take.push_back(r);
-				S->pending.pop_front();
-			}
-		}
-		const double t_admit = now_s();
-		// concatenate the admitted requests into one batch
-		int32_t n = 0;
-		int64_t bytes = 0;
-		for (auto &r : take) n += r->n, bytes += (int64_t)r->seqs.size();
-		std::vector<char> seqs((size_t)bytes + 1);
-		std::vector<int64_t> offs((size_t)n);
-		std::vector<int32_t> ql((size_t)n), v0((size_t)n), dist((size_t)n), status((size_t)n);
-		int32_t v1 = take.empty() ? -1 : take[0]->v1;
-		bool mixed_v1 = false;
-		{
-			int64_t o = 0;
-			int32_t i = 0;
-			for (auto &r : take) {
-				r->t_admit = t_admit;
-				if (r->v1 != v1) mixed_v1 = true;
-				memcpy(seqs.data() + o, r->seqs.data(), r->seqs.size());
-				for (int32_t j = 0; j < r->n; ++j, ++i)
-					offs[(size_t)i] = o + r->offs[(size_t)j], ql[(size_t)i] = r->ql[(size_t)j],
-					v0[(size_t)i] = r->v0[(size_t)j];
-				o += (int64_t)r->seqs.size();
-			}
-		}
-		int rc = 0;
-		if (mixed_v1) {
-			// requests with different v1 run one after the other
-			int32_t i = 0;
-			for (auto &r : take) {
-				rc = gwf_batch_load(*E, B, r->n, r->seqs.data(), r->offs.data(), r->ql.data(), r->v0.data(), r->v1);
-				if (!rc) rc = gwf_batch_exec(*E, *S->G, B, GWF_MODE_PERSISTENT, S->flags, 0, nullptr, nullptr);
-				if (!rc) rc = gwf_batch_fetch(*E, B, dist.data() + i, status.data() + i);
-				if (rc) break;
-				i += r->n;
-			}
-		} else {
-			rc = gwf_batch_load(*E, B, n, seqs.data(), offs.data(), ql.data(), v0.data(), v1);
-			if (!rc) rc = gwf_batch_exec(*E, *S->G, B, GWF_MODE_PERSISTENT, S->flags, 0, nullptr, nullptr);
-			if (!rc) rc = gwf_batch_fetch(*E, B, dist.data(), status.data());
-		}
-		const double t_done = now_s();
-		{
-			std::lock_guard<std::mutex> lk(S->mu);
-			int32_t i = 0;
-			for (auto &r : take) {
-				r->dist.assign(dist.begin() + i, dist.begin() + i + r->n);
-				r->status.assign(status.begin() + i, status.begin() + i + r->n);
-				if (rc) std::fill(r->status.begin(), r->status.end(), rc);
-				r->error = rc;
-				r->t_done = t_done;
-				r->done = true;
-				i += r->n;
-			}
-		}
+	const gwfb::Caps c = gwfb::caps_for(ql, level, S->G->dens_milli);
+	return gwfb::srv_al256(gwfb::srv_qbytes(ql) + gwfb::ws_layout(c).total);
+}
+
+// Called with S->mu held.
+void finish_read(gwf_srv_s *S, const std::shared_ptr<Request> &r, int32_t i, int32_t dist, int32_t st)
+{
+	r->dist[(size_t)i] = st == 0 ? dist : -1;
+	r->status[(size_t)i] = st;
+	if (++r->n_done == r->n) {
+		r->t_done = now_s();
+		r->done = true;
 		S->cv_done.notify_all();
 	}
-	B.release();
 }
+
+void release_slot(gwf_srv_s *S, int32_t tag)
+{
+	Slot &sl = S->slots[(size_t)tag];
+	sl.r.reset();
+	sl.off = -1;
+	S->free_slots.push_back(tag);
+	--S->in_flight;
+}
+
+// Fails every read that has not completed (device error). Called with S->mu held.
+void fail_all(gwf_srv_s *S, int32_t code)
+{
+	S->fatal = code;
+	for (size_t t = 0; t < S->slots.size(); ++t)
+		if (S->slots[t].r) finish_read(S, S->slots[t].r, S->slots[t].read, -1, code);
+	for (auto &r : S->pending)
+		while (r->next_read < r->n) finish_read(S, r, r->next_read++, -1, code);
+	S->pending.clear();
+	S->retry.clear();
+}
+
+// Drains completion records. Called with S->mu held; returns the number consumed.
+int drain(gwf_srv_s *S)
+{
+	int n = 0;
+	for (;;) {
+		volatile SrvDone *d = S->cq + (S->cq_pos & (S->ccap - 1));
+		if (d->gen != (int32_t)((S->cq_pos >> S->cq_shift) + 1)) break;
+		std::atomic_thread_fence(std::memory_order_acquire);
+		const int32_t tag = d->tag, dist = d->dist, st = d->status;
+		++S->cq_pos, ++n;
+		if (tag < 0 || (size_t)tag >= S->slots.size() || !S->slots[(size_t)tag].r) {
+			fail_all(S, GWF_E_CUDA);
+			gwf_set_error("gwf_srv: completion record for an unknown slot");
+			return n;
+		}
+		Slot &sl = S->slots[(size_t)tag];
+		S->pool.release(sl.off, sl.bytes);
+		sl.off = -1;
+		if (st == GWF_E_CAPACITY && sl.level < kMaxLevel) {
+			++sl.level;
+			++S->retries;
+			S->retry.push_back(tag); // keeps its slot; re-admitted with a larger arena
+			continue;
+		}
+		finish_read(S, sl.r, sl.read, dist, st);
+		release_slot(S, tag);
+	}
+	return n;
+}
+
+// Admits retries, then new reads, while slots and arena memory last; copies their bases and
+// publishes their queue entries. Called with S->mu held; returns the number published.
+int admit(gwf_srv_s *S)
+{
+	std::vector<int32_t> batch;
+	const uint64_t first = S->q_pos;
+	auto place = [&](int32_t tag) -> int {
+		Slot &sl = S->slots[(size_t)tag];
+		const int32_t ql = sl.r->ql[(size_t)sl.read];
+		const int64_t bytes = arena_bytes(S, ql, sl.level);
+		if (bytes > S->pool.cap()) return -1; // can never fit
+		const int64_t off = S->pool.alloc(bytes);
+		if (off < 0) return 0;
+		sl.off = off, sl.bytes = bytes;
+		return 1;
+	};
+	while (!S->retry.empty()) {
+		const int32_t tag = S->retry.front();
+		const int rc = place(tag);
+		if (rc == 0) break;
+		S->retry.pop_front();
+		if (rc < 0) {
+			Slot &sl = S->slots[(size_t)tag];
+			finish_read(S, sl.r, sl.read, -1, GWF_E_CAPACITY);
+			release_slot(S, tag);
+			continue;
+		}
+		batch.push_back(tag);
+	}
+	while (S->retry.empty() && !S->pending.empty() && !S->free_slots.empty()) {
+		auto r = S->pending.front();
+		const int32_t i = r->next_read;
+		if (r->ql[(size_t)i] <= 0) {
+			finish_read(S, r, i, -1, GWF_E_BAD_INPUT);
+		} else {
+			const int32_t tag = S->free_slots.back();
+			Slot &sl = S->slots[(size_t)tag];
+			sl.r = r, sl.read = i, sl.level = 0;
+			const int rc = place(tag);
+			if (rc == 0) {
+				sl.r.reset();
+				break; // wait for arena memory
+			}
+			S->free_slots.pop_back();
+			++S->in_flight;
+			if (rc < 0) {
+				finish_read(S, r, i, -1, GWF_E_CAPACITY);
+				release_slot(S, tag);
+			} else {
+				batch.push_back(tag);
+			}
+		}
+		if (r->t_admit == 0) r->t_admit = now_s();
+		if (++r->next_read == r->n) S->pending.pop_front();
+	}
+	if (batch.empty()) return 0;
+	for (int32_t tag : batch) {
+		const Slot &sl = S->slots[(size_t)tag];
+		const Request &r = *sl.r;
+		const int32_t ql = r.ql[(size_t)sl.read];
+		uint8_t *raw = (uint8_t *)S->pool_mem.p + sl.off + 256 + gwfb::srv_pk_bytes(ql);
+		if (cudaMemcpyAsync(raw, r.seqs.data() + r.offs[(size_t)sl.read], (size_t)ql, cudaMemcpyHostToDevice,
+		                    S->fstream) != cudaSuccess)
+			return -1;
+		SrvEntry &e = S->h_q[S->q_pos & (S->qcap - 1)];
+		memset(&e, 0, sizeof e);
+		e.seq = (uint32_t)(S->q_pos + 1);
+		e.tag = tag;
+		e.arena_off = sl.off;
+		e.arena_bytes = sl.bytes;
+		e.ql = ql;
+		e.v0 = r.v0[(size_t)sl.read];
+		e.v1 = r.v1;
+		e.level = sl.level;
+		++S->q_pos;
+	}
+	// queue entries (two copies when the range wraps), then the tail that publishes them
+	const uint64_t mask = S->qcap - 1;
+	for (uint64_t p = first; p < S->q_pos;) {
+		const uint64_t i = p & mask;
+		const uint64_t n = std::min<uint64_t>(S->q_pos - p, S->qcap - i);
+		if (cudaMemcpyAsync((SrvEntry *)S->q_mem.p + i, S->h_q + i, n * sizeof(SrvEntry), cudaMemcpyHostToDevice,
+		                    S->fstream) != cudaSuccess)
+			return -1;
+		p += n;
+	}
+	*S->h_tail = S->q_pos;
+	if (cudaMemcpyAsync(q_tail_dev(S), S->h_tail, 8, cudaMemcpyHostToDevice, S->fstream) != cudaSuccess ||
+	    cudaStreamSynchronize(S->fstream) != cudaSuccess) // pinned sources are reused next round
+		return -1;
+	return (int)batch.size();
+}
+
+int launch(gwf_srv_s *S)
+{
+	gwfb::SrvParams p;
+	memset(&p, 0, sizeof p);
+	p.g = S->G->view();
+	p.q = (const SrvEntry *)S->q_mem.p;
+	p.q_tail = q_tail_dev(S);
+	p.q_head = q_head_dev(S);
+	p.stop = stop_dev(S);
+	p.busy = busy_dev(S);
+	p.cq_tail = cq_tail_dev(S);
+	p.cq = S->cq_dev;
+	p.err = S->err_dev;
+	p.arena = (uint8_t *)S->pool_mem.p;
+	p.qmask = S->qcap - 1;
+	p.cmask = S->ccap - 1;
+	p.cq_shift = S->cq_shift;
+	p.dens_milli = S->G->dens_milli;
+	p.flags = S->flags;
+	p.idle_ns = kIdleNs;
+	p.max_idle_ns = kMaxIdleNs;
+	if (gwf_launch_serve(p, S->ctas, 256, S->kstream) != cudaSuccess) return -1;
+	if (cudaEventRecord(S->kdone, S->kstream) != cudaSuccess) return -1;
+	S->kernel_running = true;
+	++S->launches;
+	return 0;
+}
+
+void pump_main(gwf_srv_s *S)
+{
+	cudaSetDevice(S->device);
+	std::unique_lock<std::mutex> lk(S->mu);
+	for (;;) {
+		int progress = 0;
+		if (!S->fatal) {
+			progress += drain(S);
+			if (*S->err) {
+				fail_all(S, GWF_E_CUDA);
+				gwf_set_error("gwf_srv: device queue error");
+			}
+		}
+		if (!S->fatal) {
+			const int a = admit(S);
+			if (a < 0) {
+				cudaGetLastError();
+				fail_all(S, GWF_E_CUDA);
+				gwf_set_error("gwf_srv: copy to the device failed");
+			}
+			progress += a > 0 ? a : 0;
+		}
+		if (!S->fatal && S->kernel_running) {
+			const cudaError_t e = cudaEventQuery(S->kdone);
+			if (e == cudaSuccess) {
+				S->kernel_running = false;
+				progress += drain(S); // every claimed read has its record now
+			} else if (e != cudaErrorNotReady) {
+				cudaGetLastError();
+				fail_all(S, GWF_E_CUDA);
+				gwf_set_errorf("gwf_srv: kernel failed: %s", cudaGetErrorString(e));
+			}
+		}
+		if (!S->fatal && !S->kernel_running && S->q_pos > S->cq_pos) {
+			if (launch(S)) {
+				cudaGetLastError();
+				fail_all(S, GWF_E_CUDA);
+				gwf_set_error("gwf_srv: kernel launch failed");
+			}
+		}
+		const bool idle = S->pending.empty() && S->in_flight == 0;
+		if (S->stop && (idle || S->fatal)) break;
+		if (!progress) S->cv_work.wait_for(lk, std::chrono::microseconds(idle ? 2000 : 50));
+	}
+	lk.unlock();
+	// end the kernel: idle warps see the stop word at their next poll
+	*S->h_stop = 1;
+	cudaMemcpyAsync(stop_dev(S), S->h_stop, 4, cudaMemcpyHostToDevice, S->fstream);
+	cudaStreamSynchronize(S->fstream);
+	cudaStreamSynchronize(S->kstream);
+	cudaGetLastError();
+}
+
+void destroy_resources(gwf_srv_s *S)
+{
+	if (S->kstream) cudaStreamDestroy(S->kstream);
+	if (S->fstream) cudaStreamDestroy(S->fstream);
+	if (S->kdone) cudaEventDestroy(S->kdone);
+	S->pool_mem.release(), S->q_mem.release(), S->ctl.release();
+	if (S->mapped) cudaFreeHost(S->mapped);
+	if (S->pinned) cudaFreeHost(S->pinned);
+	cudaGetLastError();
+}
+
+uint32_t pow2_at_least(int64_t x)
+{
+	uint32_t p = 1;
+	while ((int64_t)p < x && p < (1u << 30)) p <<= 1;
+	return p;
+}
+
+} // namespace
 
 extern "C" gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t *opt)
 {
@@ -160,29 +446,47 @@ extern "C" gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t 
 	size_t fr = 0, tot = 0;
 	cudaMemGetInfo(&fr, &tot);
 	S->budget = opt && opt->arena_budget_bytes > 0 ? opt->arena_budget_bytes : (int64_t)(fr / 4);
-	S->max_reads = opt && opt->max_inflight_reads > 0 ? opt->max_inflight_reads : 65536;
-	const int n_lanes = 4;
-	for (int i = 0; i < n_lanes; ++i) {
-		Engine *E = new Engine;
-		E->device = dev;
-		if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess ||
-		    cudaEventCreate(&E->ev0) != cudaSuccess || cudaEventCreate(&E->ev1) != cudaSuccess) {
-			cudaGetLastError();
-			gwf_set_error("gwf_srv_create: stream creation failed");
-			delete E;
-			break;
-		}
-		cudaDeviceGetAttribute(&E->sm_count, cudaDevAttrMultiProcessorCount, dev);
-		Engine *ref = gwf_engine(dev);
-		E->persistent_ctas_per_sm = ref ? ref->persistent_ctas_per_sm : 1;
-		E->mem_budget = ref ? ref->mem_budget / n_lanes : ((int64_t)1 << 30);
-		S->engines.push_back(E);
+	const int32_t max_reads = opt && opt->max_inflight_reads > 0 ? opt->max_inflight_reads : 16384;
+	S->qcap = pow2_at_least(2LL * max_reads);
+	S->ccap = S->qcap;
+	while ((1u << S->cq_shift) < S->ccap) ++S->cq_shift;
+	cudaDeviceGetAttribute(&S->sm_count, cudaDevAttrMultiProcessorCount, dev);
+	S->ctas = S->sm_count * gwf_serve_ctas_per_sm();
+	bool ok = cudaStreamCreateWithFlags(&S->kstream, cudaStreamNonBlocking) == cudaSuccess &&
+	          cudaStreamCreateWithFlags(&S->fstream, cudaStreamNonBlocking) == cudaSuccess &&
+	          cudaEventCreateWithFlags(&S->kdone, cudaEventDisableTiming) == cudaSuccess;
+	ok = ok && S->pool_mem.ensure((size_t)S->budget) == 0 && S->q_mem.ensure(sizeof(SrvEntry) * S->qcap) == 0 &&
+	     S->ctl.ensure(256) == 0;
+	const size_t mapped_bytes = sizeof(SrvDone) * S->ccap + 256;
+	const size_t pinned_bytes = sizeof(SrvEntry) * S->qcap + 256;
+	ok = ok && cudaHostAlloc(&S->mapped, mapped_bytes, cudaHostAllocMapped) == cudaSuccess;
+	ok = ok && cudaHostAlloc(&S->pinned, pinned_bytes, cudaHostAllocDefault) == cudaSuccess;
+	if (ok) {
+		memset(S->mapped, 0, mapped_bytes);
+		memset(S->pinned, 0, pinned_bytes);
+		void *dp = nullptr;
+		ok = cudaHostGetDevicePointer(&dp, S->mapped, 0) == cudaSuccess;
+		S->cq = (volatile SrvDone *)S->mapped;
+		S->err = (volatile int32_t *)((char *)S->mapped + sizeof(SrvDone) * S->ccap);
+		S->cq_dev = (SrvDone *)dp;
+		S->err_dev = (int32_t *)((char *)dp + sizeof(SrvDone) * S->ccap);
+		S->h_q = (SrvEntry *)S->pinned;
+		S->h_tail = (unsigned long long *)((char *)S->pinned + sizeof(SrvEntry) * S->qcap);
+		S->h_stop = (int32_t *)(S->h_tail + 1);
 	}
-	if (S->engines.empty()) {
+	ok = ok && cudaMemsetAsync(S->ctl.p, 0, 256, S->fstream) == cudaSuccess &&
+	     cudaStreamSynchronize(S->fstream) == cudaSuccess;
+	if (!ok) {
+		cudaGetLastError();
+		gwf_set_errorf("gwf_srv_create: device set-up failed (arena budget %lld bytes)", (long long)S->budget);
+		destroy_resources(S);
 		delete S;
 		return nullptr;
 	}
-	for (int i = 0; i < (int)S->engines.size(); ++i) S->lanes.emplace_back(lane_main, S, i);
+	S->pool.init(S->budget);
+	S->slots.resize((size_t)max_reads);
+	for (int32_t t = max_reads - 1; t >= 0; --t) S->free_slots.push_back(t);
+	S->pump = std::thread(pump_main, S);
 	return S;
 }
 
@@ -206,16 +510,26 @@ extern "C" int64_t gwf_srv_submit(gwf_srv_t *S, int32_t n, const char *seqs, con
 			gwf_set_error("gwf_srv_submit: negative read length");
 			return GWF_E_BAD_INPUT;
 		}
+		if (v0[i] < 0 || (uint32_t)v0[i] >= S->G->n_vtx) {
+			gwf_set_error("gwf_srv_submit: v0 out of range");
+			return GWF_E_BAD_INPUT;
+		}
 		r->offs[(size_t)i] = tot, tot += ql[i];
 	}
-	r->seqs.resize((size_t)tot + 1);
+	r->seqs.resize((size_t)tot + 16);
 	for (int32_t i = 0; i < n; ++i) memcpy(r->seqs.data() + r->offs[(size_t)i], seqs + offs[i], (size_t)ql[i]);
 	r->ql.assign(ql, ql + n);
 	r->v0.assign(v0, v0 + n);
+	r->dist.assign((size_t)n, -1);
+	r->status.assign((size_t)n, 0);
 	r->t_submit = now_s();
 	{
 		std::lock_guard<std::mutex> lk(S->mu);
 		if (S->stop) return GWF_E_BUSY;
+		if (S->fatal) {
+			gwf_set_error("gwf_srv_submit: the server stopped after a device error");
+			return S->fatal;
+		}
 		r->id = S->next_id++;
 		S->all[r->id] = r;
 		S->pending.push_back(r);
@@ -265,6 +579,16 @@ extern "C" int gwf_srv_times(gwf_srv_t *S, int64_t req, double *t_submit, double
 	return 0;
 }
 
+extern "C" int gwf_srv_stats(gwf_srv_t *S, int64_t *launches, int64_t *retries, int64_t *arena_used)
+{
+	if (!S) return GWF_E_BAD_INPUT;
+	std::lock_guard<std::mutex> lk(S->mu);
+	if (launches) *launches = S->launches;
+	if (retries) *retries = S->retries;
+	if (arena_used) *arena_used = S->pool.used();
+	return 0;
+}
+
 extern "C" void gwf_srv_destroy(gwf_srv_t *S)
 {
 	if (!S) return;
@@ -273,7 +597,7 @@ extern "C" void gwf_srv_destroy(gwf_srv_t *S)
 		S->stop = true;
 	}
 	S->cv_work.notify_all();
-	for (auto &t : S->lanes) t.join();
-	for (Engine *E : S->engines) delete E;
+	if (S->pump.joinable()) S->pump.join();
+	destroy_resources(S);
 	delete S;
 }

@@ -147,11 +147,16 @@ int gwf_ed_batch_noalloc(const gwf_graph_t *g, int32_t n, int32_t max_ql, const 
 void *gwf_pinned_alloc(int64_t bytes);
 void gwf_pinned_free(void *p);
 
-/* ---- serving: continuous batching on a resident graph ---- */
+/* ---- serving: continuous batching on a resident graph ----
+ * No reference counterpart. One resident kernel aligns reads pulled from a device queue, one
+ * warp per read. Reads of queued requests are admitted in FIFO order while a slot is free and
+ * the arena budget holds the read's wavefront arena (sized for its own length); a read that
+ * overflows its arena is queued again in a 4x larger one, up to three times, ahead of new
+ * reads. Results equal those of gwf_ed_batch for the same reads, whatever else is in flight. */
 typedef struct gwf_srv_s gwf_srv_t;
 typedef struct {
-	int64_t arena_budget_bytes; /* device bytes for in-flight wavefront arenas */
-	int32_t max_inflight_reads; /* slots of the running kernel; 0 = derived from the budget */
+	int64_t arena_budget_bytes; /* device bytes for in-flight wavefront arenas; 0 = 1/4 of free */
+	int32_t max_inflight_reads; /* reads admitted at once (queued or running); 0 = 16384 */
 	int32_t flags;              /* GWF_F_* */
 	int32_t device;
 	int32_t reserved[7];
@@ -165,8 +170,10 @@ int64_t gwf_srv_submit(gwf_srv_t *s, int32_t n, const char *seqs, const int64_t 
 int gwf_srv_poll(gwf_srv_t *s, int64_t req, int32_t *dist, int32_t *status);
 /* Waits at most timeout_s seconds. Returns 1 done, GWF_E_TIMEOUT, or another error. */
 int gwf_srv_wait(gwf_srv_t *s, int64_t req, int32_t *dist, int32_t *status, double timeout_s);
-/* Completion and admission timestamps (seconds, steady clock) of a finished request. */
+/* Submit, first-admission and completion times (seconds, steady clock) of a finished request. */
 int gwf_srv_times(gwf_srv_t *s, int64_t req, double *t_submit, double *t_admit, double *t_done);
+/* Kernel launches so far, reads re-queued in a larger arena, arena bytes in use. */
+int gwf_srv_stats(gwf_srv_t *s, int64_t *launches, int64_t *retries, int64_t *arena_used);
 void gwf_srv_destroy(gwf_srv_t *s);
 
 /* ---- GFA input side (reference gfa-io.c, gfa-base.c, gfa-sub.c, main.cu:294-359) ---- */
