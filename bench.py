@@ -57,6 +57,16 @@ def shard_seed(workload, rank):
     return None if rank == 0 else 1000 + 17 * rank
 
 
+def reduce_max(x, dist=None, device="cuda"):
+    """Max of a per-rank timing over all ranks (the rank's own value without a process group)."""
+    if dist is None or not dist.is_initialized():
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 class ClockSampler:
     """nvidia-smi clocks during the timed region (one sample every 200 ms)."""
 
@@ -359,11 +369,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, "cuda")
 
     for _ in range(args.warmup):
         batch.run(mode=mode, ctas_per_sm=args.ctas_per_sm)
