@@ -259,7 +259,7 @@ class Graph:
             raise GwfError(r, last_error())
         return r
 
-    def ed_batch(self, reads, v0, v1=-1, mode=MODE_AUTO, flags=0, concat=True, max_lag=0):
+    def ed_batch(self, reads, v0, v1=-1, mode=MODE_AUTO, flags=0, concat=True, max_lag=0, use_graph=0):
         """Batch alignment. reads: list of bytes, or (cat, offs, lens). Returns (dist, status)."""
         if isinstance(reads, tuple):
             cat, offs, lens = reads
@@ -269,7 +269,7 @@ class Graph:
         v0 = np.ascontiguousarray(np.broadcast_to(np.asarray(v0, dtype=np.int32), (n,)))
         dist = np.zeros(n, dtype=np.int32)
         st = np.zeros(n, dtype=np.int32)
-        opt = BatchOpts(mode=mode, flags=flags)
+        opt = BatchOpts(mode=mode, flags=flags, use_graph=use_graph)
         if concat:
             rc = lib().gwf_ed_batch_concat(self.ptr, n, _ptr(cat), _ptr(offs), _ptr(lens), _ptr(v0), v1,
                                            max_lag, _ptr(dist), _ptr(st), ctypes.byref(opt))
@@ -295,9 +295,10 @@ class ResidentBatch:
         if not self.ptr:
             raise GwfError(GWF_E_CUDA, last_error())
 
-    def run(self, mode=None, flags=None, ctas_per_sm=0):
+    def run(self, mode=None, flags=None, ctas_per_sm=0, use_graph=0):
         opt = BatchOpts(mode=self.opt.mode if mode is None else mode,
-                        flags=self.opt.flags if flags is None else flags, ctas_per_sm=ctas_per_sm)
+                        flags=self.opt.flags if flags is None else flags, ctas_per_sm=ctas_per_sm,
+                        use_graph=use_graph)
         ms = ctypes.c_float(0)
         rc = lib().gwf_batch_run(self.ptr, ctypes.byref(opt), ctypes.byref(ms))
         if rc != 0:

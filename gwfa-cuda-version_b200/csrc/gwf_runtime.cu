@@ -304,6 +304,7 @@ void Batch::release()
 {
 	for (DBuf *b : {&raw, &raw_off, &ql, &v0, &pk, &pk_off, &pure, &dist, &status, &steps, &order_ql})
 		b->release();
+	if (gexec) cudaGraphExecDestroy(gexec), gexec = nullptr;
 }
 
 // Copies n reads (host, concatenated) into the batch's device buffers; computes host-side
@@ -312,6 +313,7 @@ int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64
                    const int32_t *ql, const int32_t *v0, int32_t v1)
 {
 	B.n = n, B.v1 = v1;
+	++B.generation;
 	B.h_ql.assign(ql, ql + n);
 	int64_t lo = 0, hi = 0;
 	if (n > 0) {
@@ -397,11 +399,17 @@ static KParams base_params(Engine &E, const GraphDev &G, Batch &B, int32_t flags
 static const int kWarpsPerCta = 8;
 static const int kMaxLevel = 3;
 
-// Persistent launch over the reads listed in d_order (device), arenas sized for ql_cap.
-static int launch_persistent(Engine &E, KParams p, const int32_t *d_order, int32_t n_order,
-                             int32_t ql_cap, int32_t level, int ctas_per_sm, int *launches)
+// Grid and arena of a persistent launch over n_order reads with arenas sized for ql_cap: as many
+// warps as the grid holds (at most one per read), fewer when the arenas would not fit the budget.
+struct PersistPlan {
+	int ctas = 0;
+	int64_t slot = 0;
+};
+
+static int plan_persistent(Engine &E, int32_t n_order, int32_t ql_cap, int32_t level, int ctas_per_sm,
+                           int32_t dens_milli, PersistPlan *pl)
 {
-	const Caps c = caps_for(ql_cap, level, p.dens_milli);
+	const Caps c = caps_for(ql_cap, level, dens_milli);
 	const int64_t slot = ws_layout(c).total;
 	int64_t warps = (int64_t)E.sm_count * ctas_per_sm * kWarpsPerCta;
 	const int64_t need_warps = (n_order + 0LL);
@@ -417,17 +425,35 @@ static int launch_persistent(Engine &E, KParams p, const int32_t *d_order, int32
 	int rc;
 	if ((rc = E.ws.ensure((size_t)(warps * slot)))) return rc;
 	if ((rc = E.head.ensure(16))) return rc;
+	pl->ctas = (int)(warps / kWarpsPerCta);
+	pl->slot = slot;
+	return 0;
+}
+
+static int enqueue_persistent(Engine &E, KParams p, const PersistPlan &pl, const int32_t *d_order,
+                              int32_t n_order, int32_t ql_cap, int32_t level)
+{
 	CK(cudaMemsetAsync(E.head.p, 0, 4, E.stream));
 	p.order = d_order;
 	p.n_order = n_order;
 	p.head = (int32_t *)E.head.p;
 	p.ws = (uint8_t *)E.ws.p;
-	p.slot_bytes = slot;
+	p.slot_bytes = pl.slot;
 	p.level = level;
 	p.ql_cap = ql_cap;
-	const int ctas = (int)(warps / kWarpsPerCta);
-	k_align_persistent<<<ctas, 32 * kWarpsPerCta, 0, E.stream>>>(p);
+	k_align_persistent<<<pl.ctas, 32 * kWarpsPerCta, 0, E.stream>>>(p);
 	CK(cudaGetLastError());
+	return 0;
+}
+
+// Persistent launch over the reads listed in d_order (device), arenas sized for ql_cap.
+static int launch_persistent(Engine &E, KParams p, const int32_t *d_order, int32_t n_order,
+                             int32_t ql_cap, int32_t level, int ctas_per_sm, int *launches)
+{
+	PersistPlan pl;
+	int rc;
+	if ((rc = plan_persistent(E, n_order, ql_cap, level, ctas_per_sm, p.dens_milli, &pl))) return rc;
+	if ((rc = enqueue_persistent(E, p, pl, d_order, n_order, ql_cap, level))) return rc;
 	++*launches;
 	return 0;
 }
@@ -473,8 +499,59 @@ static int launch_plain(Engine &E, KParams p, Batch &B, int *launches)
 	return 0;
 }
 
+static int enqueue_pack(Engine &E, Batch &B)
+{
+	const int ctas = (B.n + kWarpsPerCta - 1) / kWarpsPerCta;
+	k_pack_reads<<<ctas, 32 * kWarpsPerCta, 0, E.stream>>>(
+	    (const uint8_t *)B.raw.p, (const int64_t *)B.raw_off.p, (const int32_t *)B.ql.p,
+	    (const int64_t *)B.pk_off.p, (uint64_t *)B.pk.p, (uint8_t *)B.pure.p, B.n);
+	CK(cudaGetLastError());
+	return 0;
+}
+
+// Level-0 sequence of the persistent form as one CUDA graph: pack, clear the overflow count,
+// persistent kernel, copy the overflow count to the host. Captured once per batch contents and
+// launch shape, replayed on every run.
+static int launch_level0_graph(Engine &E, Batch &B, const KParams &p, int ctas_per_sm)
+{
+	PersistPlan pl;
+	int rc;
+	if ((rc = plan_persistent(E, B.n, B.max_ql, 0, ctas_per_sm, p.dens_milli, &pl))) return rc;
+	const uint64_t key[8] = {B.generation, (uint64_t)(uintptr_t)E.ws.p, (uint64_t)pl.slot, (uint64_t)pl.ctas,
+	                         (uint64_t)(uint32_t)p.flags, (uint64_t)(uintptr_t)E.retry_n.p,
+	                         (uint64_t)(uintptr_t)E.h_small.p, (uint64_t)(uintptr_t)E.retry_list.p};
+	if (!B.gexec || memcmp(key, B.gkey, sizeof key) != 0) {
+		if (B.gexec) cudaGraphExecDestroy(B.gexec), B.gexec = nullptr;
+		CK(cudaStreamBeginCapture(E.stream, cudaStreamCaptureModeThreadLocal));
+		int erc = enqueue_pack(E, B);
+		if (!erc && cudaMemsetAsync(E.retry_n.p, 0, 4, E.stream) != cudaSuccess) erc = GWF_E_CUDA;
+		if (!erc) erc = enqueue_persistent(E, p, pl, (const int32_t *)B.order_ql.p, B.n, B.max_ql, 0);
+		if (!erc && cudaMemcpyAsync(E.h_small.p, E.retry_n.p, 4, cudaMemcpyDeviceToHost, E.stream) != cudaSuccess)
+			erc = GWF_E_CUDA;
+		cudaGraph_t graph = nullptr;
+		const cudaError_t ce = cudaStreamEndCapture(E.stream, &graph);
+		if (erc || ce != cudaSuccess) {
+			if (graph) cudaGraphDestroy(graph);
+			cudaGetLastError();
+			gwf_set_error("capturing the batch launch sequence failed");
+			return erc ? erc : GWF_E_CUDA;
+		}
+		const cudaError_t ie = cudaGraphInstantiate(&B.gexec, graph, 0);
+		cudaGraphDestroy(graph);
+		if (ie != cudaSuccess) {
+			B.gexec = nullptr;
+			cudaGetLastError();
+			gwf_set_errorf("instantiating the batch graph failed: %s", cudaGetErrorString(ie));
+			return GWF_E_CUDA;
+		}
+		memcpy(B.gkey, key, sizeof key);
+	}
+	CK(cudaGraphLaunch(B.gexec, E.stream));
+	return 0;
+}
+
 int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t flags,
-                   int ctas_per_sm, float *ms, int *launches_out)
+                   int ctas_per_sm, float *ms, int *launches_out, int use_graph)
 {
 	int launches = 0, rc;
 	if (B.n == 0) {
@@ -485,25 +562,27 @@ int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t
 	if ((rc = E.retry_list.ensure(4 * (size_t)B.n + 4)) || (rc = E.retry_n.ensure(16)) ||
 	    (rc = E.h_small.ensure(4 * (size_t)B.n + 64)))
 		return rc;
-	CK(cudaEventRecord(E.ev0, E.stream));
-	{
-		const int ctas = (B.n + kWarpsPerCta - 1) / kWarpsPerCta;
-		k_pack_reads<<<ctas, 32 * kWarpsPerCta, 0, E.stream>>>(
-		    (const uint8_t *)B.raw.p, (const int64_t *)B.raw_off.p, (const int32_t *)B.ql.p,
-		    (const int64_t *)B.pk_off.p, (uint64_t *)B.pk.p, (uint8_t *)B.pure.p, B.n);
-		CK(cudaGetLastError());
-		++launches;
-	}
-	CK(cudaMemsetAsync(E.retry_n.p, 0, 4, E.stream));
 	KParams p = base_params(E, G, B, flags);
 	if (ctas_per_sm <= 0) ctas_per_sm = E.persistent_ctas_per_sm;
-	if (mode == GWF_MODE_PLAIN) rc = launch_plain(E, p, B, &launches);
-	else rc = launch_persistent(E, p, (const int32_t *)B.order_ql.p, B.n, B.max_ql, 0, ctas_per_sm, &launches);
-	if (rc) return rc;
+	bool count_copied = false;
+	CK(cudaEventRecord(E.ev0, E.stream));
+	if (use_graph && mode != GWF_MODE_PLAIN) {
+		if ((rc = launch_level0_graph(E, B, p, ctas_per_sm))) return rc;
+		launches += 2;
+		count_copied = true;
+	} else {
+		if ((rc = enqueue_pack(E, B))) return rc;
+		++launches;
+		CK(cudaMemsetAsync(E.retry_n.p, 0, 4, E.stream));
+		if (mode == GWF_MODE_PLAIN) rc = launch_plain(E, p, B, &launches);
+		else rc = launch_persistent(E, p, (const int32_t *)B.order_ql.p, B.n, B.max_ql, 0, ctas_per_sm, &launches);
+		if (rc) return rc;
+	}
 	// re-run arena overflows at larger size classes
 	for (int level = 1; level <= kMaxLevel; ++level) {
 		int32_t nr = 0;
-		CK(cudaMemcpyAsync(E.h_small.p, E.retry_n.p, 4, cudaMemcpyDeviceToHost, E.stream));
+		if (!count_copied) CK(cudaMemcpyAsync(E.h_small.p, E.retry_n.p, 4, cudaMemcpyDeviceToHost, E.stream));
+		count_copied = false;
 		CK(cudaStreamSynchronize(E.stream));
 		nr = *(int32_t *)E.h_small.p;
 		if (nr == 0) break;
@@ -609,7 +688,8 @@ extern "C" int gwf_ed_batch_concat(const gwf_graph_t *g, int32_t n, const char *
 	const int32_t mode = opt ? opt->mode : GWF_MODE_AUTO;
 	const int32_t flags = opt ? opt->flags : 0;
 	const int32_t cps = opt ? opt->ctas_per_sm : 0;
-	if ((rc = gwf_batch_exec(*E, *G, *B, mode, flags, cps, nullptr, nullptr))) return rc;
+	if ((rc = gwf_batch_exec(*E, *G, *B, mode, flags, cps, nullptr, nullptr, opt ? opt->use_graph : 0)))
+		return rc;
 	std::vector<int32_t> st;
 	if (!status) st.resize((size_t)n), status = st.data();
 	return gwf_batch_fetch(*E, *B, dist, status);
@@ -702,7 +782,7 @@ extern "C" int gwf_batch_run(gwf_batch_t *b, const gwf_batch_opts_t *opt, float 
 	if (rc) return rc;
 	std::lock_guard<std::mutex> lk(g_batch_mu);
 	return gwf_batch_exec(*E, *G, b->B, opt ? opt->mode : GWF_MODE_AUTO, opt ? opt->flags : 0,
-	                      opt ? opt->ctas_per_sm : 0, kernel_ms, &b->launches);
+	                      opt ? opt->ctas_per_sm : 0, kernel_ms, &b->launches, opt ? opt->use_graph : 0);
 }
 
 extern "C" int gwf_batch_results(gwf_batch_t *b, int32_t *dist, int32_t *status)

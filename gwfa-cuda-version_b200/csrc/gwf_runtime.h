@@ -47,6 +47,9 @@ struct Engine { // per-device launch state: stream, events, warp arenas
 struct Batch { // reads resident on the device
 	int32_t n = 0, v1 = -1, max_ql = 0;
 	int64_t pk_words = 0;
+	uint64_t generation = 0;          // bumped by every load (graph key)
+	cudaGraphExec_t gexec = nullptr;  // captured level-0 sequence of the persistent form
+	uint64_t gkey[8] = {};
 	std::vector<int32_t> h_ql, h_order;
 	std::vector<int64_t> h_raw_off, h_pk_off;
 	DBuf raw, raw_off, ql, v0, pk, pk_off, pure, dist, status, steps, order_ql;
@@ -59,7 +62,7 @@ int gwf_select_device(int want, int *dev_out);
 int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64_t *offs,
                    const int32_t *ql, const int32_t *v0, int32_t v1);
 int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t flags,
-                   int ctas_per_sm, float *ms, int *launches_out);
+                   int ctas_per_sm, float *ms, int *launches_out, int use_graph = 0);
 int gwf_batch_fetch(Engine &E, Batch &B, int32_t *dist, int32_t *status);
 namespace gwfb {
 struct KParams;

@@ -128,3 +128,26 @@ def test_resident_batch_runs_are_repeatable(G):
     assert ms > 0 and np.array_equal(d1, d2)
     assert b.launches() >= 2
     assert (b.steps() == d1 + 1).all()
+
+
+def test_graph_captured_runs_equal_stream_runs(G):
+    """use_graph = 1: the level-0 sequence (pack, persistent kernel, overflow count) replays as one
+    CUDA graph; results equal the stream-launched run, across replays and with arena retries
+    (reads unrelated to the graph overflow the first arena class)."""
+    w = G.load_workload("config1", n=300)
+    g = _indexed(G, w["graph"])
+    rng = np.random.default_rng(4)
+    junk = [bytes(rng.choice(list(b"ACGT"), size=600).astype(np.uint8)) for _ in range(4)]
+    reads = [bytes(w["cat"][o:o + l]) for o, l in zip(w["offs"], w["lens"])] + junk
+    v0 = np.concatenate([w["v0"], np.zeros(len(junk), np.int32)]).astype(np.int32)
+    cat, offs, lens = G.pack_reads(reads)
+    b = G.ResidentBatch(g, cat, offs, lens, v0)
+    b.run(use_graph=0)
+    d0, s0 = b.results()
+    for _ in range(3):
+        b.run(use_graph=1)
+        d1, s1 = b.results()
+        assert np.array_equal(d0, d1) and np.array_equal(s0, s1)
+    d2, s2 = g.ed_batch((cat, offs, lens), v0, use_graph=1)
+    assert np.array_equal(d0, d2) and np.array_equal(s0, s2)
+    b.close()
