@@ -81,6 +81,10 @@ SIGNATURES = {
     "gwf_batch_steps": (ctypes.c_int, [P, P]),
     "gwf_batch_destroy": (None, [P]),
     "gwf_ed_batch_noalloc": (ctypes.c_int, [PG, I32, I32, P, P, P, P, I32, P, P, I32, P]),
+    "gwf_tune": (ctypes.c_int, [PG, I32, P, P, P, P, I32, I32, ctypes.c_char_p]),
+    "gwf_tune_load": (ctypes.c_int, [ctypes.c_char_p, I32]),
+    "gwf_tune_get": (ctypes.c_int, [I32, I32, P, P, P]),
+    "gwf_tune_clear": (None, [I32]),
     "gwf_pinned_alloc": (P, [I64]),
     "gwf_pinned_free": (None, [P]),
     "gwf_srv_create": (P, [PG, P]),
@@ -280,6 +284,43 @@ class Graph:
         if rc != 0:
             raise GwfError(rc, last_error())
         return dist, st
+
+
+TUNE_BUCKET_MAX = (1500, 3000, 6000, 12000, None)  # upper ql bound (exclusive) per bucket
+
+
+def tune(graph, reads, v0, v1=-1, max_reads_per_bucket=0, json_path=None):
+    """gwf_tune: times the launch shapes per read-length bucket on these reads and keeps the
+    fastest for GWF_MODE_AUTO. reads: list of bytes or (cat, offs, lens). Returns tune_table()."""
+    cat, offs, lens = reads if isinstance(reads, tuple) else pack_reads(reads)
+    n = len(lens)
+    v0 = np.ascontiguousarray(np.broadcast_to(np.asarray(v0, dtype=np.int32), (n,)))
+    rc = lib().gwf_tune(graph.ptr, n, _ptr(cat), _ptr(offs), _ptr(lens), _ptr(v0), v1, max_reads_per_bucket,
+                        json_path.encode() if json_path else None)
+    if rc != 0:
+        raise GwfError(rc, last_error())
+    return tune_table()
+
+
+def tune_load(json_path, device=-1):
+    rc = lib().gwf_tune_load(json_path.encode(), device)
+    if rc != 0:
+        raise GwfError(rc, last_error())
+    return tune_table(device)
+
+
+def tune_table(device=-1):
+    """{bucket: (form, ctas_per_sm, reads_per_s)} for the buckets with an entry."""
+    out = {}
+    for b in range(len(TUNE_BUCKET_MAX)):
+        f, c, r = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_float()
+        if lib().gwf_tune_get(device, b, ctypes.byref(f), ctypes.byref(c), ctypes.byref(r)) == 1:
+            out[b] = (f.value, c.value, r.value)
+    return out
+
+
+def tune_clear(device=-1):
+    lib().gwf_tune_clear(device)
 
 
 class ResidentBatch:

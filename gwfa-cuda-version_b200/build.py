@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgwfa_b200.so")
-SOURCES = ["gwf_runtime.cu", "gwf_serve.cu", "gwf_noalloc.cu", "gfa_loader.cpp", "synth.cpp"]
+SOURCES = ["gwf_runtime.cu", "gwf_serve.cu", "gwf_tune.cu", "gwf_noalloc.cu", "gfa_loader.cpp", "synth.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

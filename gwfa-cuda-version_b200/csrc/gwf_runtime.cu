@@ -335,6 +335,11 @@ int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64
 	B.max_ql = 0;
 	for (int32_t i = 0; i < n; ++i) B.max_ql = std::max(B.max_ql, ql[i]);
 	{
+		double w[GWF_TUNE_NBUCKETS] = {0};
+		for (int32_t i = 0; i < n; ++i) w[gwf_tune_bucket(ql[i])] += (double)ql[i] * (double)ql[i];
+		B.dom_bucket = (int32_t)(std::max_element(w, w + GWF_TUNE_NBUCKETS) - w);
+	}
+	{
 		const int32_t nb = (B.max_ql >> 6) + 1;
 		std::vector<int32_t> cnt((size_t)nb + 1, 0);
 		for (int32_t i = 0; i < n; ++i) cnt[(size_t)(nb - 1 - (ql[i] >> 6)) + 1]++;
@@ -563,6 +568,10 @@ int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t
 	    (rc = E.h_small.ensure(4 * (size_t)B.n + 64)))
 		return rc;
 	KParams p = base_params(E, G, B, flags);
+	if (mode == GWF_MODE_AUTO && ctas_per_sm <= 0) { // autotuned shape for the dominant length bucket
+		int32_t f = 0, c = 0;
+		if (gwf_tune_lookup(E.device, B.dom_bucket, &f, &c)) mode = f, ctas_per_sm = c;
+	}
 	if (ctas_per_sm <= 0) ctas_per_sm = E.persistent_ctas_per_sm;
 	bool count_copied = false;
 	CK(cudaEventRecord(E.ev0, E.stream));
@@ -642,6 +651,7 @@ int gwf_serve_ctas_per_sm()
 
 // ------------------------------------------------------------------ public batch entry points
 static std::mutex g_batch_mu; // batch calls are serialised (one engine per device)
+std::mutex &gwf_batch_mutex() { return g_batch_mu; }
 static std::unordered_map<int, Batch *> g_scratch_batches;
 
 static int prepare(const gwf_graph_t *g, const gwf_batch_opts_t *opt, GraphDev **G, Engine **E)

@@ -48,6 +48,7 @@ struct Batch { // reads resident on the device
 	int32_t n = 0, v1 = -1, max_ql = 0;
 	int64_t pk_words = 0;
 	uint64_t generation = 0;          // bumped by every load (graph key)
+	int32_t dom_bucket = 0;           // length bucket with the largest sum of ql^2 (autotuner)
 	cudaGraphExec_t gexec = nullptr;  // captured level-0 sequence of the persistent form
 	uint64_t gkey[8] = {};
 	std::vector<int32_t> h_ql, h_order;
@@ -71,3 +72,8 @@ struct SrvParams;
 cudaError_t gwf_launch_persistent(const gwfb::KParams &p, int ctas, int threads, cudaStream_t s);
 cudaError_t gwf_launch_serve(const gwfb::SrvParams &p, int ctas, int threads, cudaStream_t s);
 int gwf_serve_ctas_per_sm();
+
+#include <mutex>
+std::mutex &gwf_batch_mutex();   // serialises batch calls (one engine per device)
+int gwf_tune_bucket(int32_t ql); // autotuner length bucket of a read
+int gwf_tune_lookup(int device, int32_t bucket, int32_t *form, int32_t *ctas_per_sm);

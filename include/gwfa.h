@@ -45,7 +45,7 @@ typedef struct {
 #define GWF_E_BAD_GRAPH     (-7) /* zero-length vertex, arc overlap >= target length, bad CSR */
 #define GWF_E_TIMEOUT       (-8) /* a bounded device/host wait gave up (serving loop) */
 #define GWF_E_NOMEM         (-9) /* device or host allocation failed */
-#define GWF_E_BUSY          (-10) /* serving admission refused: arena budget exhausted */
+#define GWF_E_BUSY          (-10) /* serving: the server is shutting down */
 
 /* batch flags */
 #define GWF_F_EXACT_START   0x1 /* exact edit distance at the start of the read. By default the
@@ -66,9 +66,10 @@ typedef struct {
 	int32_t mode;        /* GWF_MODE_* */
 	int32_t flags;       /* GWF_F_* */
 	int32_t device;      /* CUDA device ordinal (-1 = current) */
-	int32_t warps_per_cta; /* 0 = autotuned */
-	int32_t ctas_per_sm;   /* 0 = autotuned (persistent form) */
-	int32_t use_graph;     /* 1 = capture the launch sequence in a CUDA graph (persistent) */
+	int32_t warps_per_cta; /* must be 0: one warp aligns one read, 8 warps per CTA */
+	int32_t ctas_per_sm;   /* persistent grid; 0 = the autotuned value for GWF_MODE_AUTO (see
+	                          gwf_tune), else the occupancy limit */
+	int32_t use_graph;     /* 1 = replay the persistent form's launch sequence as a CUDA graph */
 	int32_t reserved[10];
 } gwf_batch_opts_t;
 
@@ -142,6 +143,22 @@ int gwf_ed_batch_noalloc(const gwf_graph_t *g, int32_t n, int32_t max_ql, const 
                          const int64_t *d_offs, const int32_t *d_ql, const int32_t *d_v0,
                          int32_t v1, int32_t *d_dist, int32_t *d_status, int32_t flags,
                          void *stream);
+
+/* ---- autotuner (no reference counterpart) ----
+ * Times the persistent form at 1..(occupancy limit) CTAs per SM and the plain form on the given
+ * reads, separately for each read-length bucket (ql < 1500, < 3000, < 6000, < 12000, longer;
+ * at most max_reads_per_bucket evenly spread reads each, 0 = 8192), and keeps the fastest shape
+ * per bucket for the graph's device. Batch calls with mode GWF_MODE_AUTO and ctas_per_sm = 0
+ * then use the entry of the bucket holding most of the batch's work (sum of ql^2). json_path !=
+ * NULL also writes the table as JSON; gwf_tune_load reads it back (device -1 = current). The
+ * kernel aligns each read with one warp, so warps per read is not a tuned dimension. */
+#define GWF_TUNE_NBUCKETS 5
+int gwf_tune(const gwf_graph_t *g, int32_t n, const char *seqs, const int64_t *offs, const int32_t *ql,
+             const int32_t *v0, int32_t v1, int32_t max_reads_per_bucket, const char *json_path);
+int gwf_tune_load(const char *json_path, int32_t device);
+/* 1 = the bucket has an entry (form = GWF_MODE_*, ctas_per_sm, measured reads/s), 0 = none. */
+int gwf_tune_get(int32_t device, int32_t bucket, int32_t *form, int32_t *ctas_per_sm, float *reads_per_s);
+void gwf_tune_clear(int32_t device);
 
 /* Page-locked host memory for read buffers, so that batch copies run at full PCIe speed. */
 void *gwf_pinned_alloc(int64_t bytes);
