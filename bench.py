@@ -325,6 +325,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-step-seconds", type=float, default=8.0)
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="persistent grid; 0 = occupancy limit")
+    ap.add_argument("--graph", type=int, default=1, help="1 = persistent runs replay a captured CUDA graph")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--serving", action="store_true", help="serving benchmark (config5) instead")
     ap.add_argument("--serve-reads", type=int, default=12000)
     ap.add_argument("--serve-budget-gib", type=float, default=64.0)
@@ -371,8 +373,9 @@ def main():
     def max_over_ranks(x):
         return reduce_max(x, dist, "cuda")
 
+    use_graph = args.graph if mode == G.MODE_PERSISTENT else 0
     for _ in range(args.warmup):
-        batch.run(mode=mode, ctas_per_sm=args.ctas_per_sm)
+        batch.run(mode=mode, ctas_per_sm=args.ctas_per_sm, use_graph=use_graph)
     dist_gpu, status = batch.results()
     launches = 0
     times = []
@@ -382,7 +385,7 @@ def main():
         for _ in range(args.steps):
             flush.zero_()              # evict L2 between steps (256 MB > 126 MB L2)
             torch.cuda.synchronize()
-            times.append(batch.run(mode=mode, ctas_per_sm=args.ctas_per_sm))
+            times.append(batch.run(mode=mode, ctas_per_sm=args.ctas_per_sm, use_graph=use_graph))
             launches += batch.launches()
         torch.cuda.synchronize()
     barrier()
@@ -406,18 +409,17 @@ def main():
                  "forms_identical": bool(np.array_equal(d2, dist_gpu))}
 
     # end to end through the public batch call, pinned host buffers, copies in the timed region
-    out_d = np.zeros(n, np.int32)
-    out_s = np.zeros(n, np.int32)
-    for _ in range(2):
-        g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode)
     e2e_t = []
-    barrier()
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        out_d, out_s = g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode)
-        e2e_t.append(time.perf_counter() - t0)
-    barrier()
-    e2e_s = max_over_ranks(statistics.mean(e2e_t))
+    if not args.no_e2e:
+        for _ in range(2):
+            g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode)
+        barrier()
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode)
+            e2e_t.append(time.perf_counter() - t0)
+        barrier()
+    e2e_s = max_over_ranks(statistics.mean(e2e_t)) if e2e_t else None
     h2d = int(w["offs"][-1] + w["lens"][-1]) + n * (8 + 4 + 4 + 8 + 4)
     d2h = n * 8 + 4
 
@@ -426,9 +428,11 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "config": {"workload": WORKLOAD_DESC[args.workload], "reads_per_gpu": n, "form": args.mode,
+                   "cuda_graph": bool(use_graph),
                    "l2": "flushed between steps (256 MB write)", "parallelism": "reads sharded by rank, graph replicated"},
         "gbases_per_s": world * bases / (ms / 1000.0) / 1e9,
-        "e2e": {"value": world * n / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": ({"value": world * n / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+                if e2e_s else None),
         "gpu_launches": launches,
         "status_ok": bool((status == 0).all()),
         "clocks": clk.summary(),

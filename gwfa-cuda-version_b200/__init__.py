@@ -92,7 +92,7 @@ SIGNATURES = {
     "gwf_srv_poll": (ctypes.c_int, [P, I64, P, P]),
     "gwf_srv_wait": (ctypes.c_int, [P, I64, P, P, DBL]),
     "gwf_srv_times": (ctypes.c_int, [P, I64, P, P, P]),
-    "gwf_srv_stats": (ctypes.c_int, [P, P, P, P]),
+    "gwf_srv_stats": (ctypes.c_int, [P, P, I32]),
     "gwf_srv_destroy": (None, [P]),
     "gwf_gfa_load": (PG, [ctypes.c_char_p, ctypes.c_char_p]),
     "gwf_gfa_load_mem": (PG, [ctypes.c_char_p, I64, ctypes.c_char_p]),
@@ -418,13 +418,16 @@ class Server:
             raise GwfError(rc, last_error())
         return a.value, b.value, c.value
 
+    STATS = ("launches", "retries", "arena_used", "published", "completed", "in_flight", "pending_requests",
+             "kernel_running")
+
     def stats(self):
-        """dict(launches, retries, arena_used) of the serving kernel."""
-        a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
-        rc = lib().gwf_srv_stats(self.ptr, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
-        if rc != 0:
+        """The server's counters (gwf_srv_stats) as a dict."""
+        out = np.zeros(len(self.STATS), dtype=np.int64)
+        rc = lib().gwf_srv_stats(self.ptr, _ptr(out), len(out))
+        if rc < 0:
             raise GwfError(rc, last_error())
-        return {"launches": a.value, "retries": b.value, "arena_used": c.value}
+        return dict(zip(self.STATS, (int(x) for x in out)))
 
     def close(self):
         if self.ptr:

@@ -143,6 +143,8 @@ struct gwf_srv_s {
 	SrvEntry *h_q = nullptr;
 	unsigned long long *h_tail = nullptr;
 	int32_t *h_stop = nullptr;
+	char *stage = nullptr; // pinned staging of read bases on their way to the arenas
+	int64_t stage_cap = 0;
 	Pool pool;
 	std::vector<Slot> slots;
 	std::vector<int32_t> free_slots;
@@ -293,14 +295,23 @@ int admit(gwf_srv_s *S)
 		if (++r->next_read == r->n) S->pending.pop_front();
 	}
 	if (batch.empty()) return 0;
+	int64_t staged = 0;
 	for (int32_t tag : batch) {
 		const Slot &sl = S->slots[(size_t)tag];
 		const Request &r = *sl.r;
 		const int32_t ql = r.ql[(size_t)sl.read];
 		uint8_t *raw = (uint8_t *)S->pool_mem.p + sl.off + 256 + gwfb::srv_pk_bytes(ql);
-		if (cudaMemcpyAsync(raw, r.seqs.data() + r.offs[(size_t)sl.read], (size_t)ql, cudaMemcpyHostToDevice,
-		                    S->fstream) != cudaSuccess)
-			return -1;
+		const char *src = r.seqs.data() + r.offs[(size_t)sl.read];
+		if (ql <= S->stage_cap) { // through pinned staging: an asynchronous DMA
+			if (staged + ql > S->stage_cap) {
+				if (cudaStreamSynchronize(S->fstream) != cudaSuccess) return -1;
+				staged = 0;
+			}
+			memcpy(S->stage + staged, src, (size_t)ql);
+			src = S->stage + staged;
+			staged += (ql + 15) & ~15;
+		}
+		if (cudaMemcpyAsync(raw, src, (size_t)ql, cudaMemcpyHostToDevice, S->fstream) != cudaSuccess) return -1;
 		SrvEntry &e = S->h_q[S->q_pos & (S->qcap - 1)];
 		memset(&e, 0, sizeof e);
 		e.seq = (uint32_t)(S->q_pos + 1);
@@ -458,7 +469,8 @@ extern "C" gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t 
 	ok = ok && S->pool_mem.ensure((size_t)S->budget) == 0 && S->q_mem.ensure(sizeof(SrvEntry) * S->qcap) == 0 &&
 	     S->ctl.ensure(256) == 0;
 	const size_t mapped_bytes = sizeof(SrvDone) * S->ccap + 256;
-	const size_t pinned_bytes = sizeof(SrvEntry) * S->qcap + 256;
+	S->stage_cap = 64LL << 20;
+	const size_t pinned_bytes = sizeof(SrvEntry) * S->qcap + 256 + (size_t)S->stage_cap;
 	ok = ok && cudaHostAlloc(&S->mapped, mapped_bytes, cudaHostAllocMapped) == cudaSuccess;
 	ok = ok && cudaHostAlloc(&S->pinned, pinned_bytes, cudaHostAllocDefault) == cudaSuccess;
 	if (ok) {
@@ -473,6 +485,7 @@ extern "C" gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t 
 		S->h_q = (SrvEntry *)S->pinned;
 		S->h_tail = (unsigned long long *)((char *)S->pinned + sizeof(SrvEntry) * S->qcap);
 		S->h_stop = (int32_t *)(S->h_tail + 1);
+		S->stage = (char *)S->pinned + sizeof(SrvEntry) * S->qcap + 256;
 	}
 	ok = ok && cudaMemsetAsync(S->ctl.p, 0, 256, S->fstream) == cudaSuccess &&
 	     cudaStreamSynchronize(S->fstream) == cudaSuccess;
@@ -579,14 +592,15 @@ extern "C" int gwf_srv_times(gwf_srv_t *S, int64_t req, double *t_submit, double
 	return 0;
 }
 
-extern "C" int gwf_srv_stats(gwf_srv_t *S, int64_t *launches, int64_t *retries, int64_t *arena_used)
+extern "C" int gwf_srv_stats(gwf_srv_t *S, int64_t *out, int32_t n_out)
 {
-	if (!S) return GWF_E_BAD_INPUT;
+	if (!S || (n_out > 0 && !out)) return GWF_E_BAD_INPUT;
 	std::lock_guard<std::mutex> lk(S->mu);
-	if (launches) *launches = S->launches;
-	if (retries) *retries = S->retries;
-	if (arena_used) *arena_used = S->pool.used();
-	return 0;
+	const int64_t v[GWF_SRV_NSTATS] = {S->launches, S->retries, S->pool.used(), (int64_t)S->q_pos,
+	                                   (int64_t)S->cq_pos, S->in_flight, (int64_t)S->pending.size(),
+	                                   S->kernel_running ? 1 : 0};
+	for (int32_t i = 0; i < n_out && i < GWF_SRV_NSTATS; ++i) out[i] = v[i];
+	return GWF_SRV_NSTATS;
 }
 
 extern "C" void gwf_srv_destroy(gwf_srv_t *S)

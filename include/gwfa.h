@@ -189,8 +189,12 @@ int gwf_srv_poll(gwf_srv_t *s, int64_t req, int32_t *dist, int32_t *status);
 int gwf_srv_wait(gwf_srv_t *s, int64_t req, int32_t *dist, int32_t *status, double timeout_s);
 /* Submit, first-admission and completion times (seconds, steady clock) of a finished request. */
 int gwf_srv_times(gwf_srv_t *s, int64_t req, double *t_submit, double *t_admit, double *t_done);
-/* Kernel launches so far, reads re-queued in a larger arena, arena bytes in use. */
-int gwf_srv_stats(gwf_srv_t *s, int64_t *launches, int64_t *retries, int64_t *arena_used);
+/* Counters of the server, in this order: kernel launches, reads re-queued in a larger arena,
+ * arena bytes in use, queue positions published, completion records consumed, reads admitted
+ * and not finished, requests not fully admitted, kernel running (0/1). Fills min(n_out,
+ * GWF_SRV_NSTATS) values and returns GWF_SRV_NSTATS. */
+#define GWF_SRV_NSTATS 8
+int gwf_srv_stats(gwf_srv_t *s, int64_t *out, int32_t n_out);
 void gwf_srv_destroy(gwf_srv_t *s);
 
 /* ---- GFA input side (reference gfa-io.c, gfa-base.c, gfa-sub.c, main.cu:294-359) ---- */
