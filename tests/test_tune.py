@@ -42,5 +42,8 @@ def test_tuned_auto_equals_fixed_shapes(G, tmp_path):
     d_pers, s_pers = g.ed_batch(reads, w["v0"], mode=G.MODE_PERSISTENT)
     assert np.array_equal(d_auto, d_pers) and np.array_equal(s_auto, s_pers)
     G.tune_clear()
-    assert G.tune_load(path) == table
+    loaded = G.tune_load(path)
+    assert {b: v[:2] for b, v in loaded.items()} == {b: v[:2] for b, v in table.items()}
+    for b, v in table.items():
+        assert loaded[b][2] == pytest.approx(v[2], abs=0.06)  # the file keeps reads/s to 0.1
     G.tune_clear()
