@@ -328,7 +328,7 @@ def main():
     ap.add_argument("--graph", type=int, default=1, help="1 = persistent runs replay a captured CUDA graph")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--serving", action="store_true", help="serving benchmark (config5) instead")
-    ap.add_argument("--serve-reads", type=int, default=12000)
+    ap.add_argument("--serve-reads", type=int, default=6000)
     ap.add_argument("--serve-budget-gib", type=float, default=64.0)
     ap.add_argument("--plain-sample", type=int, default=6)
     args = ap.parse_args()

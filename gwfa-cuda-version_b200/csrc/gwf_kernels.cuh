@@ -63,10 +63,14 @@ struct SrvParams {
 	uint32_t qmask, cmask;
 	int32_t cq_shift;                  // log2(cmask + 1)
 	int32_t dens_milli, flags;
-	int64_t idle_ns;                   // an idle warp leaves after this when no warp is busy
-	int64_t max_idle_ns;               // and after this in any case
+	int64_t idle_ns;                   // the leader warp closes the kernel after this idle
+	                                   // time when no warp is busy
+	int64_t max_idle_ns;               // any warp closes it after this idle time
 };
 constexpr int32_t SRV_ERR_SEQ = 1;     // a claimed entry did not carry its position
+// Set in q_head when the kernel closes. Claims and the closing mark both change q_head with
+// atomicCAS, so a read is either claimed before the mark or stays queued for the next launch.
+constexpr unsigned long long SRV_CLOSED = 1ULL << 62;
 
 __host__ __device__ inline int64_t srv_al256(int64_t x) { return (x + 255) & ~255LL; }
 __host__ __device__ inline int64_t srv_pk_bytes(int32_t ql) { return srv_al256(8LL * ((ql + 31) / 32 + 2)); }
@@ -591,12 +595,16 @@ __device__ __forceinline__ int32_t ld_acquire_s32(const int32_t *p)
 // Serving form. A warp claims the next published queue position (bounded, backed-off polling of
 // device memory), packs the read that the host copied into its arena, aligns it at the entry's
 // capacity class, and writes a completion record into host-mapped memory (an arena overflow
-// comes back as GWF_E_CAPACITY; the host re-queues the read in a larger arena). Idle warps leave
-// after idle_ns once no warp holds a read, and after max_idle_ns in any case; the host relaunches
-// the kernel when work is queued and it has ended.
+// comes back as GWF_E_CAPACITY; the host re-queues the read in a larger arena).
+// The kernel ends as a whole: one leader warp marks q_head closed after idle_ns with nothing
+// queued and no warp busy (any warp does after max_idle_ns), and every warp leaves when it sees
+// the mark. A warp counts itself busy before it tries to claim, so the leader never closes
+// under a claim in progress. The host relaunches the kernel when positions are queued and it
+// has ended.
 __global__ void __launch_bounds__(256, 3) k_serve(const __grid_constant__ SrvParams p)
 {
 	const int lane = threadIdx.x & 31;
+	const bool leader = blockIdx.x == 0 && (threadIdx.x >> 5) == 0;
 	for (int64_t guard = 0; guard < (1LL << 40); ++guard) {
 		long long h = -1;
 		if (lane == 0) {
@@ -604,22 +612,27 @@ __global__ void __launch_bounds__(256, 3) k_serve(const __grid_constant__ SrvPar
 			uint32_t ns = 128;
 			for (int64_t spin = 0; spin < (1LL << 32); ++spin) {
 				if (ld_acquire_s32(p.stop)) break;
-				const unsigned long long tail = ld_acquire_u64(p.q_tail);
 				const unsigned long long head = *(volatile const unsigned long long *)p.q_head;
+				if (head & SRV_CLOSED) break;
+				const unsigned long long tail = ld_acquire_u64(p.q_tail);
 				if (head < tail) {
+					atomicAdd(p.busy, 1);
 					if (atomicCAS(p.q_head, head, head + 1) == head) {
 						h = (long long)head;
 						break;
 					}
+					atomicSub(p.busy, 1);
 					continue;
 				}
 				const int64_t idle = (int64_t)(globaltimer_ns() - t0);
-				if (idle > p.max_idle_ns) break;
-				if (idle > p.idle_ns && *(volatile const int32_t *)p.busy == 0) break;
+				if (idle > p.max_idle_ns ||
+				    (leader && idle > p.idle_ns && *(volatile const int32_t *)p.busy == 0)) {
+					atomicCAS(p.q_head, head, head | SRV_CLOSED); // fails if a read was claimed
+					continue;
+				}
 				__nanosleep(ns);
-				if (ns < 16384) ns *= 2;
+				if (ns < 32768) ns *= 2;
 			}
-			if (h >= 0) atomicAdd(p.busy, 1);
 		}
 		h = __shfl_sync(FULL, h, 0);
 		if (h < 0) break;
@@ -628,7 +641,11 @@ __global__ void __launch_bounds__(256, 3) k_serve(const __grid_constant__ SrvPar
 		const SrvEntry *ep = p.q + (h & p.qmask);
 		const uint32_t seq = __ldcg((const unsigned int *)&ep->seq);
 		if (seq != (uint32_t)(h + 1)) { // cannot happen while the host keeps its ring bounds
-			if (lane == 0) atomicOr(p.err, SRV_ERR_SEQ), atomicSub(p.busy, 1);
+			if (lane == 0) {
+				atomicOr(p.err, SRV_ERR_SEQ);
+				atomicOr(p.q_head, SRV_CLOSED);
+				atomicSub(p.busy, 1);
+			}
 			break;
 		}
 		const int32_t tag = __ldcg(&ep->tag), ql = __ldcg(&ep->ql), v0 = __ldcg(&ep->v0);

@@ -9,8 +9,8 @@
 //     the arena and the slot, and completes a request when its last read is done;
 //   * retry: a read that overflows its arena comes back with GWF_E_CAPACITY and is queued again
 //     in a 4x larger arena (up to three times), ahead of new reads;
-//   * liveness: idle warps leave after a few milliseconds once no warp is busy; the pump
-//     relaunches the kernel when positions are queued and it has ended.
+//   * liveness: the kernel closes as a whole a few milliseconds after the queue runs dry with no
+//     warp busy; the pump relaunches it when positions are queued and it has ended.
 // Reads that arrive while others are on the device therefore start as soon as a warp and arena
 // memory are free, and results do not depend on what else is in flight.
 #include <cuda_runtime.h>
@@ -47,7 +47,7 @@ double now_s()
 
 constexpr int kMaxLevel = 3;         // arena classes 1x, 4x, 16x, 64x, as the batch path
 constexpr int64_t kIdleNs = 5000000; // 5 ms
-constexpr int64_t kMaxIdleNs = 30LL * 1000000000LL;
+constexpr int64_t kMaxIdleNs = 120LL * 1000000000LL;
 
 // Best-fit allocator over [0, cap) in 256-byte units, with coalescing.
 class Pool {
@@ -141,7 +141,7 @@ struct gwf_srv_s {
 	SrvDone *cq_dev = nullptr;
 	int32_t *err_dev = nullptr;
 	SrvEntry *h_q = nullptr;
-	unsigned long long *h_tail = nullptr;
+	unsigned long long *h_tail = nullptr, *h_head = nullptr;
 	int32_t *h_stop = nullptr;
 	char *stage = nullptr; // pinned staging of read bases on their way to the arenas
 	int64_t stage_cap = 0;
@@ -164,11 +164,13 @@ struct gwf_srv_s {
 
 namespace {
 
+// control words: the ones every idle warp polls share one 128-byte line, the ones that busy
+// warps update sit on lines of their own
 unsigned long long *q_tail_dev(gwf_srv_s *S) { return (unsigned long long *)S->ctl.p; }
 unsigned long long *q_head_dev(gwf_srv_s *S) { return (unsigned long long *)S->ctl.p + 1; }
-unsigned long long *cq_tail_dev(gwf_srv_s *S) { return (unsigned long long *)S->ctl.p + 2; }
-int32_t *stop_dev(gwf_srv_s *S) { return (int32_t *)((unsigned long long *)S->ctl.p + 3); }
-int32_t *busy_dev(gwf_srv_s *S) { return stop_dev(S) + 1; }
+int32_t *stop_dev(gwf_srv_s *S) { return (int32_t *)((unsigned long long *)S->ctl.p + 2); }
+unsigned long long *cq_tail_dev(gwf_srv_s *S) { return (unsigned long long *)((char *)S->ctl.p + 128); }
+int32_t *busy_dev(gwf_srv_s *S) { return (int32_t *)((char *)S->ctl.p + 256); }
 
 int64_t arena_bytes(const gwf_srv_s *S, int32_t ql, int32_t level)
 {
@@ -343,6 +345,14 @@ int admit(gwf_srv_s *S)
 
 int launch(gwf_srv_s *S)
 {
+	// the previous kernel left q_head marked closed: clear the mark (nothing runs on the device)
+	unsigned long long head = 0;
+	if (cudaMemcpy(&head, q_head_dev(S), 8, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+	if (head & gwfb::SRV_CLOSED) {
+		*S->h_head = head & ~gwfb::SRV_CLOSED;
+		if (cudaMemcpyAsync(q_head_dev(S), S->h_head, 8, cudaMemcpyHostToDevice, S->kstream) != cudaSuccess)
+			return -1;
+	}
 	gwfb::SrvParams p;
 	memset(&p, 0, sizeof p);
 	p.g = S->G->view();
@@ -467,7 +477,7 @@ extern "C" gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t 
 	          cudaStreamCreateWithFlags(&S->fstream, cudaStreamNonBlocking) == cudaSuccess &&
 	          cudaEventCreateWithFlags(&S->kdone, cudaEventDisableTiming) == cudaSuccess;
 	ok = ok && S->pool_mem.ensure((size_t)S->budget) == 0 && S->q_mem.ensure(sizeof(SrvEntry) * S->qcap) == 0 &&
-	     S->ctl.ensure(256) == 0;
+	     S->ctl.ensure(384) == 0;
 	const size_t mapped_bytes = sizeof(SrvDone) * S->ccap + 256;
 	S->stage_cap = 64LL << 20;
 	const size_t pinned_bytes = sizeof(SrvEntry) * S->qcap + 256 + (size_t)S->stage_cap;
@@ -484,10 +494,11 @@ extern "C" gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t 
 		S->err_dev = (int32_t *)((char *)dp + sizeof(SrvDone) * S->ccap);
 		S->h_q = (SrvEntry *)S->pinned;
 		S->h_tail = (unsigned long long *)((char *)S->pinned + sizeof(SrvEntry) * S->qcap);
-		S->h_stop = (int32_t *)(S->h_tail + 1);
+		S->h_head = S->h_tail + 1;
+		S->h_stop = (int32_t *)(S->h_tail + 2);
 		S->stage = (char *)S->pinned + sizeof(SrvEntry) * S->qcap + 256;
 	}
-	ok = ok && cudaMemsetAsync(S->ctl.p, 0, 256, S->fstream) == cudaSuccess &&
+	ok = ok && cudaMemsetAsync(S->ctl.p, 0, 384, S->fstream) == cudaSuccess &&
 	     cudaStreamSynchronize(S->fstream) == cudaSuccess;
 	if (!ok) {
 		cudaGetLastError();

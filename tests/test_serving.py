@@ -103,6 +103,35 @@ def test_arena_overflow_is_retried(G):
     assert stats["retries"] > 0
 
 
+def test_kernel_closes_when_idle_and_relaunches(G):
+    """After the queue runs dry the resident kernel ends as a whole; a later request starts a new
+    launch with every warp, so it runs as fast as the first."""
+    w = G.load_workload("config3", n=600)
+    g = w["graph"]
+    g.index()
+    reads = (w["cat"], w["offs"], w["lens"])
+    srv = G.Server(g)
+    try:
+        t = []
+        for rep in range(2):
+            t0 = time.perf_counter()
+            rid, k = srv.submit(reads, w["v0"])
+            d, st = srv.wait(rid, k, timeout_s=300)
+            t.append(time.perf_counter() - t0)
+            assert (st == 0).all()
+            for _ in range(400):  # the kernel closes ~5 ms after the last read
+                if srv.stats()["kernel_running"] == 0:
+                    break
+                time.sleep(0.005)
+            assert srv.stats()["kernel_running"] == 0
+        assert srv.stats()["launches"] == 2
+        assert t[1] < 3 * t[0] + 0.5
+    finally:
+        srv.close()
+    solo, _ = g.ed_batch(reads, w["v0"])
+    assert np.array_equal(d, solo)
+
+
 def test_poll_and_unknown_request(G):
     w = G.load_workload("config1", n=8)
     g = w["graph"]
