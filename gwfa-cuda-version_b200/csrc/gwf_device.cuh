@@ -323,28 +323,10 @@ __device__ __forceinline__ bool in_ranges(const uint64_t *lo, const uint64_t *hi
 }
 
 // Warp bitonic sort of keys[0..n) with int payload; buffers hold pow2ceil(n) entries.
-__device__ inline void warp_bitonic_sort(uint64_t *keys, int32_t *vals, int32_t n)
+// Bitonic network in global memory for lists longer than 32 (kept out of line: it is rare).
+static __device__ __noinline__ void warp_bitonic_sort_global(uint64_t *keys, int32_t *vals, int32_t n)
 {
 	const int lane = threadIdx.x & 31;
-	if (n <= 1) return;
-	if (n <= 32) {
-		// one element per lane; its rank is the number of smaller keys (equal keys by lane)
-		__syncwarp();
-		const uint64_t key = lane < n ? keys[lane] : PAD_KEY;
-		const int32_t val = (vals && lane < n) ? vals[lane] : 0;
-		int32_t rank = 0;
-		for (int32_t t = 0; t < n; ++t) {
-			const uint64_t o = __shfl_sync(FULL, key, t);
-			rank += o < key || (o == key && t < lane);
-		}
-		__syncwarp();
-		if (lane < n) {
-			keys[rank] = key;
-			if (vals) vals[rank] = val;
-		}
-		__syncwarp();
-		return;
-	}
 	int32_t N = pow2ceil_i(n);
 	for (int32_t i = n + lane; i < N; i += 32) keys[i] = PAD_KEY;
 	__syncwarp();
@@ -366,6 +348,31 @@ __device__ inline void warp_bitonic_sort(uint64_t *keys, int32_t *vals, int32_t 
 			}
 			__syncwarp();
 		}
+}
+
+__device__ __forceinline__ void warp_bitonic_sort(uint64_t *keys, int32_t *vals, int32_t n)
+{
+	const int lane = threadIdx.x & 31;
+	if (n <= 1) return;
+	if (n <= 32) {
+		// one element per lane; its rank is the number of smaller keys (equal keys by lane)
+		__syncwarp();
+		const uint64_t key = lane < n ? keys[lane] : PAD_KEY;
+		const int32_t val = (vals && lane < n) ? vals[lane] : 0;
+		int32_t rank = 0;
+		for (int32_t t = 0; t < n; ++t) {
+			const uint64_t o = __shfl_sync(FULL, key, t);
+			rank += o < key || (o == key && t < lane);
+		}
+		__syncwarp();
+		if (lane < n) {
+			keys[rank] = key;
+			if (vals) vals[rank] = val;
+		}
+		__syncwarp();
+		return;
+	}
+	warp_bitonic_sort_global(keys, vals, n);
 }
 
 #endif // __CUDACC__

@@ -81,9 +81,12 @@ __host__ __device__ inline int64_t srv_qbytes(int32_t ql)
 
 #ifndef GWF_KERNELS_DECL_ONLY
 // Aligns read r with one warp. All control flow is warp-uniform.
-__device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *wsb, const Caps &c)
+// The arena capacities are those of caps_for(min(ql, ql_cap), level): the arena at wsb must hold
+// them (callers size it for ql_cap, or for the read itself).
+__device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *wsb, int32_t ql_cap, int32_t level)
 {
 	const int lane = threadIdx.x & 31;
+	const Caps c = caps_for(p.r.ql[r] < ql_cap ? p.r.ql[r] : ql_cap, level, p.dens_milli);
 	const DevGraph &g = p.g;
 	const WsOff o = ws_layout(c);
 	uint64_t *const h = (uint64_t *)(wsb + o.h);
@@ -486,44 +489,77 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 			__syncwarp();
 		} else {
 			warp_bitonic_sort(ba_vd, ba_k, n_ba);
-			// merge the in-vertex and arc-side candidates into a (ties: in-vertex first)
-			const int32_t n_m = n_x + n_ba;
-			for (int32_t j = lane; j < n_x; j += 32) {
-				const uint64_t x = x_vd[j];
-				const int32_t pos = j + lower_bound_u64(ba_vd, n_ba, x);
-				a_vd[pos] = x, a_k[pos] = x_k[j];
-			}
-			for (int32_t j = lane; j < n_ba; j += 32) {
-				const uint64_t x = ba_vd[j];
-				const int32_t pos = j + upper_bound_u64(x_vd, n_x, x);
-				a_vd[pos] = x, a_k[pos] = ba_k[j];
-			}
-			__syncwarp();
-			// keep the furthest k per diagonal, drop diagonals inside an ended interval
-			for (int32_t base = 0; base < n_m; base += 32) {
+			// 1. arc-side candidates: one per diagonal with the furthest k, minus those inside an
+			// ended interval; a diagonal also present among the in-vertex candidates folds its k
+			// into that entry (each in-vertex entry receives at most one, as the list is unique)
+			int32_t n_b = 0;
+			for (int32_t base = 0; base < n_ba; base += 32) {
 				const int32_t j = base + lane;
 				bool keep = false;
 				uint64_t vd = 0;
 				int32_t k = 0;
-				if (j < n_m) {
-					vd = a_vd[j], k = a_k[j];
-					if (j == 0 || a_vd[j - 1] != vd) {
-						for (int32_t t = j + 1; t < n_m && a_vd[t] == vd; ++t) {
-							const int32_t kt = a_k[t];
+				if (j < n_ba) {
+					vd = ba_vd[j], k = ba_k[j];
+					if (j == 0 || ba_vd[j - 1] != vd) {
+						for (int32_t t = j + 1; t < n_ba && ba_vd[t] == vd; ++t) {
+							const int32_t kt = ba_k[t];
 							k = kt > k ? kt : k;
 						}
 						keep = !in_ranges(ilo, ihi, n_i, vd, i_min, i_max);
+						if (keep) {
+							const int32_t px = upper_bound_u64(x_vd, n_x, vd);
+							if (px > 0 && x_vd[px - 1] == vd) {
+								if (k > x_k[px - 1]) x_k[px - 1] = k;
+								keep = false;
+							}
+						}
 					}
 				}
 				__syncwarp();
 				const uint32_t m = __ballot_sync(FULL, keep);
 				if (keep) {
-					const int32_t pos = n_new + __popc(m & lanemask_lt());
-					a_vd[pos] = vd, a_k[pos] = k;
+					const int32_t pos = n_b + __popc(m & lanemask_lt());
+					ba_vd[pos] = vd, ba_k[pos] = k;
 				}
-				n_new += __popc(m);
+				n_b += __popc(m);
 				__syncwarp();
 			}
+			// 2. in-vertex candidates outside the ended intervals go to their merged rank; tb
+			// keeps, per chunk of 32, the kept count before the chunk and the chunk's keep mask
+			uint64_t *const chunk = tb;
+			int32_t n_kx = 0;
+			for (int32_t base = 0; base < n_x; base += 32) {
+				const int32_t j = base + lane;
+				bool keep = false;
+				uint64_t vd = 0;
+				int32_t k = 0;
+				if (j < n_x) {
+					vd = x_vd[j], k = x_k[j];
+					keep = !in_ranges(ilo, ihi, n_i, vd, i_min, i_max);
+				}
+				const uint32_t m = __ballot_sync(FULL, keep);
+				if (lane == 0) chunk[base >> 5] = (uint64_t)(uint32_t)n_kx << 32 | m;
+				if (keep) {
+					const int32_t pos = n_kx + __popc(m & lanemask_lt()) + lower_bound_u64(ba_vd, n_b, vd);
+					a_vd[pos] = vd, a_k[pos] = k;
+				}
+				n_kx += __popc(m);
+			}
+			__syncwarp();
+			// 3. arc-side candidates after the kept in-vertex candidates below them
+			const int32_t n_chunks = (n_x + 31) >> 5;
+			for (int32_t j = lane; j < n_b; j += 32) {
+				const uint64_t vd = ba_vd[j];
+				const int32_t px = upper_bound_u64(x_vd, n_x, vd), cx = px >> 5;
+				int32_t below = n_kx;
+				if (cx < n_chunks) {
+					const uint64_t info = chunk[cx];
+					below = (int32_t)(info >> 32) + __popc((uint32_t)info & ((1u << (px & 31)) - 1));
+				}
+				a_vd[j + below] = vd, a_k[j + below] = ba_k[j];
+			}
+			n_new = n_kx + n_b;
+			__syncwarp();
 		}
 		n_a = n_new;
 		if (n_a == 0) break; // wavefront emptied: no alignment (gwf-ed.cu:1313, 1336)
@@ -550,8 +586,7 @@ __global__ void __launch_bounds__(256, 3) k_align_plain(const __grid_constant__ 
 	const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
 	if (gw >= p.n_order) return;
 	const int32_t r = p.order[gw];
-	const Caps c = caps_for(p.r.ql[r], p.level, p.dens_milli);
-	align_read(p, r, p.ws + p.slot_off[gw], c);
+	align_read(p, r, p.ws + p.slot_off[gw], p.r.ql[r], p.level);
 }
 
 // Persistent form: each warp owns one arena (sized for ql_cap) and pulls reads from the
@@ -568,8 +603,7 @@ __global__ void __launch_bounds__(256, 3) k_align_persistent(const __grid_consta
 		qi = __shfl_sync(FULL, qi, 0);
 		if (qi >= p.n_order) break;
 		const int32_t r = p.order[qi];
-		const int32_t ql = p.r.ql[r];
-		align_read(p, r, wsb, caps_for(ql < p.ql_cap ? ql : p.ql_cap, p.level, p.dens_milli));
+		align_read(p, r, wsb, p.ql_cap, p.level);
 	}
 }
 
@@ -698,7 +732,7 @@ __global__ void __launch_bounds__(256, 3) k_serve(const __grid_constant__ SrvPar
 			lp.flags = p.flags;
 			lp.dist = &hdr->dist;
 			lp.status = &hdr->status;
-			align_read(lp, 0, ab + qb, c);
+			align_read(lp, 0, ab + qb, ql, level);
 			__syncwarp();
 			dist = *(volatile int32_t *)&hdr->dist;
 			st = *(volatile int32_t *)&hdr->status;
