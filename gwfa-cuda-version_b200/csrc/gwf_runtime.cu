@@ -419,9 +419,9 @@ static int plan_persistent(Engine &E, int32_t n_order, int32_t ql_cap, int32_t l
 	int64_t warps = (int64_t)E.sm_count * ctas_per_sm * kWarpsPerCta;
 	const int64_t need_warps = (n_order + 0LL);
 	if (warps > need_warps) warps = std::max<int64_t>(kWarpsPerCta, ((need_warps + kWarpsPerCta - 1) / kWarpsPerCta) * kWarpsPerCta);
-	// keep arenas within a budget of the device memory (free memory sampled when the engine
-	// was created, plus what the arena already holds)
-	const int64_t budget = E.mem_budget + (int64_t)E.ws.cap;
+	// keep arenas within a budget of the device memory: half the memory that was free when the
+	// engine was created, or what the arena already holds if that is more
+	const int64_t budget = std::max<int64_t>(E.mem_budget, (int64_t)E.ws.cap);
 	while (warps > kWarpsPerCta && warps * slot > budget) warps -= kWarpsPerCta;
 	if (warps * slot > budget) {
 		gwf_set_errorf("arena of %lld bytes per warp does not fit the device", (long long)slot);
@@ -467,7 +467,7 @@ static int launch_persistent(Engine &E, KParams p, const int32_t *d_order, int32
 // arenas of all reads do not fit).
 static int launch_plain(Engine &E, KParams p, Batch &B, int *launches)
 {
-	const int64_t budget = E.mem_budget + (int64_t)E.ws.cap;
+	const int64_t budget = std::max<int64_t>(E.mem_budget, (int64_t)E.ws.cap);
 	int32_t start = 0;
 	std::vector<int64_t> offs;
 	while (start < B.n) {
