@@ -11,7 +11,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgwfa_b200.so")
+CLI = os.path.join(HERE, "gwf-b200")
 SOURCES = ["gwf_runtime.cu", "gwf_serve.cu", "gwf_tune.cu", "gwf_noalloc.cu", "gfa_loader.cpp", "synth.cpp"]
+# gwf_cli.cpp is the command-line driver (a separate executable, not part of the library)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -22,9 +24,9 @@ def _deps():
 
 
 def needs_build():
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(CLI):
         return True
-    t = os.path.getmtime(LIB)
+    t = min(os.path.getmtime(LIB), os.path.getmtime(CLI))
     return any(os.path.getmtime(f) > t for f in _deps())
 
 
@@ -44,6 +46,15 @@ def build(force=False, ptxas=False, verbose=False):
         raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
     if ptxas:
         print(res.stdout + res.stderr)
+    # the gwf-test compatible command-line driver, linked against the library next to it
+    cxx = os.environ.get("CXX", "g++")
+    cmd = [cxx, "-O2", "-std=c++17", "-o", CLI, os.path.join(CSRC, "gwf_cli.cpp"), "-L" + HERE, "-lgwfa_b200",
+           "-Wl,-rpath,$ORIGIN", "-lz"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("g++ failed:\n" + res.stdout + res.stderr)
     return LIB
 
 

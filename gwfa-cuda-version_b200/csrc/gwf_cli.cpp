@@ -1,0 +1,161 @@
+// gwf_cli.cpp — gwf-b200, a command-line driver with the interface of the reference's gwf-test
+// (main.cu:360-750): the same options and arguments, one edit distance per read on stdout, in
+// input order. The alignment runs through the library's batch entry point on the device.
+//
+//   gwf-b200 [-p] [-s STR] [-l INT] [-m persistent|plain] [-x] <target.gfa> <query.fa|fq[.gz]>
+//
+//   -p   print the graph (gwf_graph_print format) and exit     (main.cu:382-387, 354-359)
+//   -s   starting segment name [first]                          (main.cu:399-407)
+//   -l   max lag; accepted and ignored, as in the reference     (main.cu:371, 377)
+//   -m   execution form [persistent]
+//   -x   exact start state (GWF_F_EXACT_START)
+//
+// Every read is aligned from offset 0 of the start segment (vertex 0 of the converted graph),
+// as the reference kernel does (main.cu:217). Timing and counts go to stderr.
+#include <zlib.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gwfa.h"
+
+namespace {
+
+// FASTA/FASTQ records, plain or gzip, sequences concatenated (multi-line FASTA joined).
+bool read_seqs(const char *path, std::vector<char> &cat, std::vector<int64_t> &offs, std::vector<int32_t> &lens)
+{
+	gzFile fp = gzopen(path, "r");
+	if (!fp) return false;
+	std::vector<char> line(1 << 16);
+	std::string cur;
+	bool in_seq = false, fastq = false;
+	int fq_state = 0; // 0 header, 1 sequence, 2 plus line, 3 qualities
+	auto flush = [&]() {
+		if (!in_seq) return;
+		offs.push_back((int64_t)cat.size());
+		lens.push_back((int32_t)cur.size());
+		cat.insert(cat.end(), cur.begin(), cur.end());
+		cur.clear();
+		in_seq = false;
+	};
+	std::string buf;
+	while (gzgets(fp, line.data(), (int)line.size())) {
+		buf.append(line.data());
+		if (buf.empty() || (buf.back() != '\n' && !gzeof(fp))) continue; // long line: keep reading
+		while (!buf.empty() && (buf.back() == '\n' || buf.back() == '\r')) buf.pop_back();
+		if (fastq) {
+			if (fq_state == 0 && !buf.empty() && buf[0] == '@') fq_state = 1, in_seq = true;
+			else if (fq_state == 1) cur = buf, fq_state = 2;
+			else if (fq_state == 2) flush(), fq_state = 3;
+			else if (fq_state == 3) fq_state = 0;
+		} else if (!buf.empty() && buf[0] == '>') {
+			flush();
+			in_seq = true;
+		} else if (!buf.empty() && buf[0] == '@' && offs.empty() && !in_seq) {
+			fastq = true, fq_state = 1, in_seq = true;
+		} else if (in_seq) {
+			cur += buf;
+		}
+		buf.clear();
+	}
+	if (!fastq) flush();
+	gzclose(fp);
+	return true;
+}
+
+void usage()
+{
+	fprintf(stderr, "Usage: gwf-b200 [options] <target.gfa> <query.fa>\n");
+	fprintf(stderr, "Options:\n");
+	fprintf(stderr, "  -l INT    max lag behind the furthest wavefront; accepted and ignored [0]\n");
+	fprintf(stderr, "  -s STR    starting segment name [first]\n");
+	fprintf(stderr, "  -p        output GFA in the forward strand\n");
+	fprintf(stderr, "  -m STR    execution form: persistent or plain [persistent]\n");
+	fprintf(stderr, "  -x        exact start state (no reference start-state rule)\n");
+}
+
+} // namespace
+
+int main(int argc, char *argv[])
+{
+	bool print_graph = false, exact = false;
+	const char *sname = nullptr;
+	int32_t mode = GWF_MODE_PERSISTENT;
+	uint32_t max_lag = 0;
+	int i = 1;
+	for (; i < argc && argv[i][0] == '-' && argv[i][1]; ++i) {
+		const char *a = argv[i];
+		if (!strcmp(a, "-p")) print_graph = true;
+		else if (!strcmp(a, "-x")) exact = true;
+		else if (!strcmp(a, "-s") && i + 1 < argc) sname = argv[++i];
+		else if (!strcmp(a, "-l") && i + 1 < argc) max_lag = (uint32_t)atoi(argv[++i]);
+		else if (!strcmp(a, "-m") && i + 1 < argc) {
+			const char *m = argv[++i];
+			if (!strcmp(m, "plain")) mode = GWF_MODE_PLAIN;
+			else if (!strcmp(m, "persistent")) mode = GWF_MODE_PERSISTENT;
+			else {
+				usage();
+				return 1;
+			}
+		} else {
+			usage();
+			return 1;
+		}
+	}
+	if ((!print_graph && argc - i < 2) || (print_graph && argc - i < 1)) {
+		usage();
+		return 1;
+	}
+	gwf_graph_t *g = gwf_gfa_load(argv[i], sname);
+	if (!g) {
+		fprintf(stderr, "ERROR: %s\n", gwf_last_error());
+		return 1;
+	}
+	if (print_graph) {
+		const int64_t n = gwf_graph_dump(g, nullptr, 0);
+		std::vector<char> text((size_t)n + 1);
+		gwf_graph_dump(g, text.data(), n + 1);
+		fwrite(text.data(), 1, (size_t)n, stdout);
+		gwf_graph_free(g);
+		return 0;
+	}
+	std::vector<char> cat;
+	std::vector<int64_t> offs;
+	std::vector<int32_t> lens;
+	if (!read_seqs(argv[i + 1], cat, offs, lens)) {
+		fprintf(stderr, "ERROR: cannot read %s\n", argv[i + 1]);
+		gwf_graph_free(g);
+		return 1;
+	}
+	cat.resize(cat.size() + 16, 0);
+	const int32_t n = (int32_t)lens.size();
+	fprintf(stderr, "[gwf-b200] %d reads, %zu bases, %u vertices, %u arcs\n", n, cat.size() - 16, g->n_vtx, g->n_arc);
+	gwf_ed_index(g);
+	std::vector<int32_t> v0((size_t)n, 0), dist((size_t)n, -1), status((size_t)n, 0);
+	gwf_batch_opts_t opt;
+	memset(&opt, 0, sizeof opt);
+	opt.mode = mode;
+	opt.flags = exact ? GWF_F_EXACT_START : 0;
+	const auto t0 = std::chrono::steady_clock::now();
+	const int rc = n > 0 ? gwf_ed_batch_concat(g, n, cat.data(), offs.data(), lens.data(), v0.data(), -1, max_lag,
+	                                           dist.data(), status.data(), &opt)
+	                     : 0;
+	const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+	if (rc) {
+		fprintf(stderr, "ERROR: batch alignment failed (%d): %s\n", rc, gwf_last_error());
+		gwf_graph_free(g);
+		return 1;
+	}
+	int32_t bad = 0;
+	for (int32_t j = 0; j < n; ++j) {
+		printf("%d\n", dist[(size_t)j]);
+		if (status[(size_t)j] != GWF_OK) ++bad;
+	}
+	fprintf(stderr, "[gwf-b200] aligned in %.6f s (%d reads with a per-read error status)\n", el, bad);
+	gwf_graph_free(g);
+	return bad ? 2 : 0;
+}

@@ -38,7 +38,8 @@ typedef struct {
 #define GWF_OK               0
 #define GWF_NO_ALIGNMENT    (-1) /* distance value: wavefront emptied (gwf-ed.cu:1336) */
 #define GWF_E_BAD_INPUT     (-2) /* ql <= 0, v0/v1 out of range, null pointer */
-#define GWF_E_UNSUPPORTED   (-3) /* traceback != 0 or max_lag != 0: the reference has neither */
+#define GWF_E_UNSUPPORTED   (-3) /* traceback != 0: the reference has none (max_lag is accepted
+                                   * and ignored, as the reference ignores it) */
 #define GWF_E_CAPACITY      (-4) /* read did not fit the largest wavefront arena class */
 #define GWF_E_CUDA          (-5) /* CUDA runtime failure or no usable B200 device */
 #define GWF_E_NOT_INDEXED   (-6) /* gwf_ed_index was not called for this graph */

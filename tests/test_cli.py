@@ -1,0 +1,60 @@
+"""gwf-b200, the command-line driver with gwf-test's interface (main.cu:360-750): graph dumps
+byte-identical to the reference's `gwf-test -p`, and on a GPU the reference's own distances for
+its exposed fixture (tolerance 0: int32 distances)."""
+import gzip
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLD, PKG_DIR, read_golden
+
+CLI = os.path.join(PKG_DIR, "gwf-b200")
+
+
+def run(*args, check=True):
+    return subprocess.run([CLI, *args], capture_output=True, text=True, check=check, timeout=600)
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built(G):
+    G.lib()  # builds the library and the driver when only sources are present
+    assert os.access(CLI, os.X_OK)
+
+
+@pytest.mark.parametrize("name", ["graph_1000", "grafo_test"])
+def test_print_graph_equals_reference_dump(name):
+    out = run("-p", os.path.join(GOLD, name + ".gfa")).stdout
+    assert out == open(os.path.join(GOLD, name + ".ref_dump.txt")).read()
+
+
+def test_usage_and_bad_arguments():
+    assert run(check=False).returncode == 1
+    assert run("-m", "nope", "a.gfa", "b.fa", check=False).returncode == 1
+    r = run(os.path.join(GOLD, "missing.gfa"), os.path.join(GOLD, "reads_200.fa"), check=False)
+    assert r.returncode == 1 and "ERROR" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", ["persistent", "plain"])
+def test_scores_equal_reference_gwf_test(form, tmp_path):
+    _, ref = read_golden("ref_exposed_200.txt")
+    gfa = os.path.join(GOLD, "graph_1000.gfa")
+    reads = os.path.join(GOLD, "reads_200.fa")
+    out = run("-m", form, gfa, reads).stdout.split()
+    assert np.array_equal(np.array(out, dtype=np.int64), np.asarray(ref))
+    # the same reads gzip-compressed, as FASTQ
+    fq = tmp_path / "r.fq.gz"
+    names, seqs = [], []
+    for line in open(reads):
+        line = line.strip()
+        if line.startswith(">"):
+            names.append(line[1:]), seqs.append("")
+        elif line:
+            seqs[-1] += line
+    with gzip.open(fq, "wt") as f:
+        for n, s in zip(names, seqs):
+            f.write("@%s\n%s\n+\n%s\n" % (n, s, "I" * len(s)))
+    out2 = run(gfa, str(fq)).stdout.split()
+    assert out2 == out
