@@ -90,24 +90,45 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 	const DevGraph &g = p.g;
 	const WsOff o = ws_layout(c);
 	uint64_t *const h = (uint64_t *)(wsb + o.h);
-	uint64_t *a_vd = (uint64_t *)(wsb + o.a_vd);
-	int32_t *a_k = (int32_t *)(wsb + o.a_k);
-	uint64_t *x_vd = (uint64_t *)(wsb + o.x_vd);
-	int32_t *x_k = (int32_t *)(wsb + o.x_k);
-	uint64_t *const ba_vd = (uint64_t *)(wsb + o.ba_vd);
-	int32_t *const ba_k = (int32_t *)(wsb + o.ba_k);
-	uint64_t *e_vd = (uint64_t *)(wsb + o.w0_vd);
-	int32_t *e_k = (int32_t *)(wsb + o.w0_k);
-	uint64_t *f_vd = (uint64_t *)(wsb + o.w1_vd);
-	int32_t *f_k = (int32_t *)(wsb + o.w1_k);
-	uint64_t *const n_vd = (uint64_t *)(wsb + o.n_vd);
-	int32_t *const n_k = (int32_t *)(wsb + o.n_k);
-	uint64_t *const tb = (uint64_t *)(wsb + o.tb);
-	uint64_t *const ta = (uint64_t *)(wsb + o.ta);
-	uint64_t *const ilo = (uint64_t *)(wsb + o.i0_lo);
-	uint64_t *const ihi = (uint64_t *)(wsb + o.i0_hi);
-	uint64_t *const clo = (uint64_t *)(wsb + o.i1_lo);
-	uint64_t *const chi = (uint64_t *)(wsb + o.i1_hi);
+	// The arena's arrays, as 32-bit byte offsets from wsb (32-bit offsets hold fewer registers
+	// than 64-bit pointers); the upper-case names are the arrays.
+	uint32_t off_a_vd = (uint32_t)o.a_vd;
+	uint32_t off_x_vd = (uint32_t)o.x_vd;
+	const uint32_t off_ba_vd = (uint32_t)o.ba_vd;
+	uint32_t off_e_vd = (uint32_t)o.w0_vd;
+	uint32_t off_f_vd = (uint32_t)o.w1_vd;
+	const uint32_t off_n_vd = (uint32_t)o.n_vd;
+	const uint32_t off_tb = (uint32_t)o.tb;
+	const uint32_t off_ta = (uint32_t)o.ta;
+	const uint32_t off_ilo = (uint32_t)o.i0_lo;
+	const uint32_t off_ihi = (uint32_t)o.i0_hi;
+	const uint32_t off_clo = (uint32_t)o.i1_lo;
+	const uint32_t off_chi = (uint32_t)o.i1_hi;
+	uint32_t off_a_k = (uint32_t)o.a_k;
+	uint32_t off_x_k = (uint32_t)o.x_k;
+	const uint32_t off_ba_k = (uint32_t)o.ba_k;
+	uint32_t off_e_k = (uint32_t)o.w0_k;
+	uint32_t off_f_k = (uint32_t)o.w1_k;
+	const uint32_t off_n_k = (uint32_t)o.n_k;
+#define A_VD ((uint64_t *)(wsb + off_a_vd))
+#define X_VD ((uint64_t *)(wsb + off_x_vd))
+#define BA_VD ((uint64_t *)(wsb + off_ba_vd))
+#define E_VD ((uint64_t *)(wsb + off_e_vd))
+#define F_VD ((uint64_t *)(wsb + off_f_vd))
+#define N_VD ((uint64_t *)(wsb + off_n_vd))
+#define TB ((uint64_t *)(wsb + off_tb))
+#define TA ((uint64_t *)(wsb + off_ta))
+#define ILO ((uint64_t *)(wsb + off_ilo))
+#define IHI ((uint64_t *)(wsb + off_ihi))
+#define CLO ((uint64_t *)(wsb + off_clo))
+#define CHI ((uint64_t *)(wsb + off_chi))
+#define A_K ((int32_t *)(wsb + off_a_k))
+#define X_K ((int32_t *)(wsb + off_x_k))
+#define BA_K ((int32_t *)(wsb + off_ba_k))
+#define E_K ((int32_t *)(wsb + off_e_k))
+#define F_K ((int32_t *)(wsb + off_f_k))
+#define N_K ((int32_t *)(wsb + off_n_k))
+
 
 	ReadCtx rc;
 	rc.ql = p.r.ql[r];
@@ -125,6 +146,10 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 		if (lane == 0) p.dist[r] = -1, p.status[r] = ST_BAD_INPUT;
 		return;
 	}
+	if (o.total > 0xffffffffLL) { // the 32-bit offsets above (caps_for keeps arenas below 4 GB)
+		if (lane == 0) p.dist[r] = -1, p.status[r] = ST_CAPACITY;
+		return;
+	}
 
 	// clear the arrival set (16-byte stores; h is 16-byte aligned, c.h is a power of two >= 256)
 	{
@@ -132,7 +157,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 		const uint4 z = make_uint4(0, 0, 0, 0);
 		for (int32_t i = lane; i < c.h / 2; i += 32) h4[i] = z;
 	}
-	if (lane == 0) a_vd[0] = gen_vd((uint32_t)v0, 0), a_k[0] = -1; // gwf-ed.cu:1303-1308
+	if (lane == 0) A_VD[0] = gen_vd((uint32_t)v0, 0), A_K[0] = -1; // gwf-ed.cu:1303-1308
 	__syncwarp();
 	const uint32_t hmask = (uint32_t)c.h - 1;
 	const int32_t hlimit = c.h - c.h / 4;
@@ -157,12 +182,12 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 			uint64_t vd = 0;
 			int32_t k = 0;
 			if (j < n_a) {
-				vd = a_vd[j];
-				k = a_k[j];
+				vd = A_VD[j];
+				k = A_K[j];
 				const uint32_t v = vd_v(vd);
 				const int32_t d = vd_d(vd), vl = (int32_t)__ldg(g.len + v);
 				k = ext(g, rc, v, d, k, vl);
-				a_k[j] = k;
+				A_K[j] = k;
 				const bool vend = k == vl - 1, qend = d + k == ql - 1;
 				if (qend) {
 					if (v1 < 0 || ((int32_t)v == v1 && vend)) found = true;
@@ -172,7 +197,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 			}
 			const uint32_t m = __ballot_sync(FULL, toE);
 			const int32_t pos = n_e + __popc(m & lanemask_lt());
-			if (toE && pos < c.w) e_vd[pos] = vd, e_k[pos] = k;
+			if (toE && pos < c.w) E_VD[pos] = vd, E_K[pos] = k;
 			n_e += __popc(m);
 		}
 		if (__any_sync(FULL, found)) {
@@ -191,13 +216,13 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 			int32_t ck[3];
 			bool keep[3] = {false, false, false}, tmp[3] = {false, false, false};
 			if (j < n_a) {
-				const uint64_t vd = a_vd[j];
-				const int32_t k = a_k[j];
+				const uint64_t vd = A_VD[j];
+				const int32_t k = A_K[j];
 				const int32_t vl = (int32_t)__ldg(g.len + vd_v(vd));
-				const uint64_t pv = j > 0 ? a_vd[j - 1] : 0;
-				const int32_t pk = j > 0 ? a_k[j - 1] : 0;
-				const uint64_t nv = j + 1 < n_a ? a_vd[j + 1] : 0;
-				const int32_t nk = j + 1 < n_a ? a_k[j + 1] : 0;
+				const uint64_t pv = j > 0 ? A_VD[j - 1] : 0;
+				const int32_t pk = j > 0 ? A_K[j - 1] : 0;
+				const uint64_t nv = j + 1 < n_a ? A_VD[j + 1] : 0;
+				const int32_t nk = j + 1 < n_a ? A_K[j + 1] : 0;
 				const bool left_in = j > 0 && pv == vd - 1, left2 = j > 0 && pv == vd - 2;
 				const bool right_in = j + 1 < n_a && nv == vd + 1, right2 = j + 1 < n_a && nv == vd + 2;
 				bool has[3];
@@ -235,7 +260,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 #pragma unroll
 				for (int t = 0; t < 3; ++t)
 					if (keep[t]) {
-						if (off < c.x) x_vd[off] = cv[t], x_k[off] = ck[t];
+						if (off < c.x) X_VD[off] = cv[t], X_K[off] = ck[t];
 						++off;
 					}
 				n_x += __popc(k0) + __popc(k1) + __popc(k2);
@@ -246,7 +271,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 #pragma unroll
 					for (int t = 0; t < 3; ++t)
 						if (tmp[t]) {
-							if (offt < c.tb) tb[offt] = cv[t];
+							if (offt < c.tb) TB[offt] = cv[t];
 							++offt;
 						}
 					n_tb += __popc(t0) + __popc(t1) + __popc(t2);
@@ -272,7 +297,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				int32_t k = 0, d = 0, vl = 0, i = 0, nv = 0;
 				uint32_t v = 0, aoff = 0;
 				if (act) {
-					vd = e_vd[j], k = e_k[j];
+					vd = E_VD[j], k = E_K[j];
 					v = vd_v(vd), d = vd_d(vd), vl = (int32_t)__ldg(g.len + v), i = d + k;
 					isq = i == ql - 1;
 					isv = !isq;
@@ -284,7 +309,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				{
 					const uint32_t m = __ballot_sync(FULL, isv);
 					const int32_t pos = n_ta + __popc(m & lanemask_lt());
-					if (isv && pos < c.ta) ta[pos] = vd;
+					if (isv && pos < c.ta) TA[pos] = vd;
 					n_ta += __popc(m);
 				}
 				const int32_t max_nv = __reduce_max_sync(FULL, (uint32_t)nv);
@@ -311,17 +336,17 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 					}
 					const uint32_t me = __ballot_sync(FULL, enter);
 					const int32_t pe = n_n + __popc(me & lanemask_lt());
-					if (enter && pe < c.w) n_vd[pe] = gen_vd(w, i + 1 - ol), n_k[pe] = ol;
+					if (enter && pe < c.w) N_VD[pe] = gen_vd(w, i + 1 - ol), N_K[pe] = ol;
 					n_n += __popc(me);
 					int32_t tot;
 					int32_t pb = warp_excl_scan(two ? 2 : (one ? 1 : 0), &tot) + n_ba;
 					if (two) {
 						if (pb + 1 < c.ba) {
-							ba_vd[pb] = gen_vd(w, i - ol), ba_k[pb] = ol;         // deletion
-							ba_vd[pb + 1] = gen_vd(w, i + 1 - ol), ba_k[pb + 1] = ol; // mismatch
+							BA_VD[pb] = gen_vd(w, i - ol), BA_K[pb] = ol;         // deletion
+							BA_VD[pb + 1] = gen_vd(w, i + 1 - ol), BA_K[pb + 1] = ol; // mismatch
 						}
 					} else if (one) {
-						if (pb < c.ba) ba_vd[pb] = gen_vd(w, i - ol), ba_k[pb] = ol;
+						if (pb < c.ba) BA_VD[pb] = gen_vd(w, i - ol), BA_K[pb] = ol;
 					}
 					n_ba += tot;
 				}
@@ -332,8 +357,8 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				const uint32_t mi = __ballot_sync(FULL, ins || qdel);
 				const int32_t pi = n_ba + __popc(mi & lanemask_lt());
 				if ((ins || qdel) && pi < c.ba) {
-					ba_vd[pi] = ins ? gen_vd(v, d + 1) : gen_vd(v, d - 1);
-					ba_k[pi] = ins ? k : k + 1;
+					BA_VD[pi] = ins ? gen_vd(v, d + 1) : gen_vd(v, d - 1);
+					BA_K[pi] = ins ? k : k + 1;
 				}
 				n_ba += __popc(mi);
 			}
@@ -357,7 +382,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				int32_t k = 0, d = 0;
 				uint32_t v = 0;
 				if (j < n_n) {
-					vd = n_vd[j], k = n_k[j];
+					vd = N_VD[j], k = N_K[j];
 					v = vd_v(vd), d = vd_d(vd);
 					const int32_t vl = (int32_t)__ldg(g.len + v);
 					k = ext(g, rc, v, d, k, vl);
@@ -372,14 +397,14 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				}
 				const uint32_t mf = __ballot_sync(FULL, toF);
 				const int32_t pf = n_f + __popc(mf & lanemask_lt());
-				if (toF && pf < c.w) f_vd[pf] = vd, f_k[pf] = k;
+				if (toF && pf < c.w) F_VD[pf] = vd, F_K[pf] = k;
 				n_f += __popc(mf);
 				const uint32_t m3 = __ballot_sync(FULL, three);
 				const int32_t p3 = n_ba + 3 * __popc(m3 & lanemask_lt());
 				if (three && p3 + 2 < c.ba) {
-					ba_vd[p3] = gen_vd(v, d - 1), ba_k[p3] = k + 1;     // deletion
-					ba_vd[p3 + 1] = gen_vd(v, d), ba_k[p3 + 1] = k + 1; // mismatch
-					ba_vd[p3 + 2] = gen_vd(v, d + 1), ba_k[p3 + 2] = k; // insertion
+					BA_VD[p3] = gen_vd(v, d - 1), BA_K[p3] = k + 1;     // deletion
+					BA_VD[p3 + 1] = gen_vd(v, d), BA_K[p3 + 1] = k + 1; // mismatch
+					BA_VD[p3 + 2] = gen_vd(v, d + 1), BA_K[p3 + 2] = k; // insertion
 				}
 				n_ba += 3 * __popc(m3);
 			}
@@ -389,9 +414,8 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				break;
 			}
 			__syncwarp();
-			uint64_t *tv = e_vd;
-			int32_t *tk = e_k;
-			e_vd = f_vd, e_k = f_k, f_vd = tv, f_k = tk;
+			const uint32_t tv = off_e_vd, tk = off_e_k;
+			off_e_vd = off_f_vd, off_e_k = off_f_k, off_f_vd = tv, off_f_k = tk;
 			n_e = n_f;
 		}
 		if (__any_sync(FULL, found)) {
@@ -407,7 +431,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 		// ---- phase 4: ended-diagonal intervals, then the next wavefront
 		// (gwf_dedup / gwf_intv_merge2 / gwf_diag_dedup / gwf_mixed_dedup, gwf-ed.cu:780-804)
 		if (n_tb + n_ta > 0) {
-			warp_bitonic_sort(ta, nullptr, n_ta);
+			warp_bitonic_sort(TA, nullptr, n_ta);
 			// rank-merge the old ranges with both point lists, ties ordered I < TB < TA
 			const int32_t n_c = n_i + n_tb + n_ta;
 			if (n_c > c.iv + c.tb + c.ta) {
@@ -415,19 +439,19 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				break;
 			}
 			for (int32_t j = lane; j < n_i; j += 32) {
-				const uint64_t x = ilo[j];
-				const int32_t pos = j + lower_bound_u64(tb, n_tb, x) + lower_bound_u64(ta, n_ta, x);
-				clo[pos] = x, chi[pos] = ihi[j];
+				const uint64_t x = ILO[j];
+				const int32_t pos = j + lower_bound_u64(TB, n_tb, x) + lower_bound_u64(TA, n_ta, x);
+				CLO[pos] = x, CHI[pos] = IHI[j];
 			}
 			for (int32_t j = lane; j < n_tb; j += 32) {
-				const uint64_t x = tb[j];
-				const int32_t pos = j + upper_bound_u64(ilo, n_i, x) + lower_bound_u64(ta, n_ta, x);
-				clo[pos] = x, chi[pos] = x + 1;
+				const uint64_t x = TB[j];
+				const int32_t pos = j + upper_bound_u64(ILO, n_i, x) + lower_bound_u64(TA, n_ta, x);
+				CLO[pos] = x, CHI[pos] = x + 1;
 			}
 			for (int32_t j = lane; j < n_ta; j += 32) {
-				const uint64_t x = ta[j];
-				const int32_t pos = j + upper_bound_u64(ilo, n_i, x) + upper_bound_u64(tb, n_tb, x);
-				clo[pos] = x, chi[pos] = x + 1;
+				const uint64_t x = TA[j];
+				const int32_t pos = j + upper_bound_u64(ILO, n_i, x) + upper_bound_u64(TB, n_tb, x);
+				CLO[pos] = x, CHI[pos] = x + 1;
 			}
 			__syncwarp();
 			// coalesce overlapping or touching ranges (gwf_intv_merge_adj, gwf-ed.cu:266-296)
@@ -436,21 +460,21 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 			for (int32_t base = 0; base < n_c; base += 32) {
 				const int32_t j = base + lane;
 				const bool act = j < n_c;
-				const uint64_t lo = act ? clo[j] : 0, hi = act ? chi[j] : 0;
+				const uint64_t lo = act ? CLO[j] : 0, hi = act ? CHI[j] : 0;
 				uint64_t pm = warp_incl_max(hi);
 				if (base > 0 && carry > pm) pm = carry;
 				uint64_t prev = __shfl_up_sync(FULL, pm, 1);
 				if (lane == 0) prev = carry;
 				const bool start = act && (j == 0 || lo > prev);
-				const bool end = act && (j + 1 == n_c || clo[j + 1] > pm);
+				const bool end = act && (j + 1 == n_c || CLO[j + 1] > pm);
 				const uint32_t ms = __ballot_sync(FULL, start);
 				if (start) {
 					const int32_t rk = n_new + __popc(ms & lanemask_lt());
-					if (rk < c.iv) ilo[rk] = lo;
+					if (rk < c.iv) ILO[rk] = lo;
 				}
 				if (end) {
 					const int32_t rk = n_new + __popc(ms & (lanemask_lt() | (1u << lane))) - 1;
-					if (rk < c.iv) ihi[rk] = pm;
+					if (rk < c.iv) IHI[rk] = pm;
 				}
 				n_new += __popc(ms);
 				carry = __shfl_sync(FULL, pm, 31);
@@ -461,7 +485,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				break;
 			}
 			__syncwarp();
-			i_min = ilo[0], i_max = ihi[n_i - 1];
+			i_min = ILO[0], i_max = IHI[n_i - 1];
 		}
 		int32_t n_new = 0;
 		if (n_ba == 0) {
@@ -473,22 +497,21 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				int32_t k = 0;
 				bool keep = false;
 				if (j < n_x) {
-					vd = x_vd[j], k = x_k[j];
-					keep = !in_ranges(ilo, ihi, n_i, vd, i_min, i_max);
+					vd = X_VD[j], k = X_K[j];
+					keep = !in_ranges(ILO, IHI, n_i, vd, i_min, i_max);
 				}
 				const uint32_t m = __ballot_sync(FULL, keep);
 				if (keep) {
 					const int32_t pos = n_new + __popc(m & lanemask_lt());
-					x_vd[pos] = vd, x_k[pos] = k;
+					X_VD[pos] = vd, X_K[pos] = k;
 				}
 				n_new += __popc(m);
 			}
-			uint64_t *tv = a_vd;
-			int32_t *tk = a_k;
-			a_vd = x_vd, a_k = x_k, x_vd = tv, x_k = tk;
+			const uint32_t tv = off_a_vd, tk = off_a_k;
+			off_a_vd = off_x_vd, off_a_k = off_x_k, off_x_vd = tv, off_x_k = tk;
 			__syncwarp();
 		} else {
-			warp_bitonic_sort(ba_vd, ba_k, n_ba);
+			warp_bitonic_sort(BA_VD, BA_K, n_ba);
 			// 1. arc-side candidates: one per diagonal with the furthest k, minus those inside an
 			// ended interval; a diagonal also present among the in-vertex candidates folds its k
 			// into that entry (each in-vertex entry receives at most one, as the list is unique)
@@ -499,17 +522,17 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				uint64_t vd = 0;
 				int32_t k = 0;
 				if (j < n_ba) {
-					vd = ba_vd[j], k = ba_k[j];
-					if (j == 0 || ba_vd[j - 1] != vd) {
-						for (int32_t t = j + 1; t < n_ba && ba_vd[t] == vd; ++t) {
-							const int32_t kt = ba_k[t];
+					vd = BA_VD[j], k = BA_K[j];
+					if (j == 0 || BA_VD[j - 1] != vd) {
+						for (int32_t t = j + 1; t < n_ba && BA_VD[t] == vd; ++t) {
+							const int32_t kt = BA_K[t];
 							k = kt > k ? kt : k;
 						}
-						keep = !in_ranges(ilo, ihi, n_i, vd, i_min, i_max);
+						keep = !in_ranges(ILO, IHI, n_i, vd, i_min, i_max);
 						if (keep) {
-							const int32_t px = upper_bound_u64(x_vd, n_x, vd);
-							if (px > 0 && x_vd[px - 1] == vd) {
-								if (k > x_k[px - 1]) x_k[px - 1] = k;
+							const int32_t px = upper_bound_u64(X_VD, n_x, vd);
+							if (px > 0 && X_VD[px - 1] == vd) {
+								if (k > X_K[px - 1]) X_K[px - 1] = k;
 								keep = false;
 							}
 						}
@@ -519,14 +542,14 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				const uint32_t m = __ballot_sync(FULL, keep);
 				if (keep) {
 					const int32_t pos = n_b + __popc(m & lanemask_lt());
-					ba_vd[pos] = vd, ba_k[pos] = k;
+					BA_VD[pos] = vd, BA_K[pos] = k;
 				}
 				n_b += __popc(m);
 				__syncwarp();
 			}
-			// 2. in-vertex candidates outside the ended intervals go to their merged rank; tb
+			// 2. in-vertex candidates outside the ended intervals go to their merged rank; TB
 			// keeps, per chunk of 32, the kept count before the chunk and the chunk's keep mask
-			uint64_t *const chunk = tb;
+			uint64_t *const chunk = TB;
 			int32_t n_kx = 0;
 			for (int32_t base = 0; base < n_x; base += 32) {
 				const int32_t j = base + lane;
@@ -534,14 +557,14 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				uint64_t vd = 0;
 				int32_t k = 0;
 				if (j < n_x) {
-					vd = x_vd[j], k = x_k[j];
-					keep = !in_ranges(ilo, ihi, n_i, vd, i_min, i_max);
+					vd = X_VD[j], k = X_K[j];
+					keep = !in_ranges(ILO, IHI, n_i, vd, i_min, i_max);
 				}
 				const uint32_t m = __ballot_sync(FULL, keep);
 				if (lane == 0) chunk[base >> 5] = (uint64_t)(uint32_t)n_kx << 32 | m;
 				if (keep) {
-					const int32_t pos = n_kx + __popc(m & lanemask_lt()) + lower_bound_u64(ba_vd, n_b, vd);
-					a_vd[pos] = vd, a_k[pos] = k;
+					const int32_t pos = n_kx + __popc(m & lanemask_lt()) + lower_bound_u64(BA_VD, n_b, vd);
+					A_VD[pos] = vd, A_K[pos] = k;
 				}
 				n_kx += __popc(m);
 			}
@@ -549,14 +572,14 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 			// 3. arc-side candidates after the kept in-vertex candidates below them
 			const int32_t n_chunks = (n_x + 31) >> 5;
 			for (int32_t j = lane; j < n_b; j += 32) {
-				const uint64_t vd = ba_vd[j];
-				const int32_t px = upper_bound_u64(x_vd, n_x, vd), cx = px >> 5;
+				const uint64_t vd = BA_VD[j];
+				const int32_t px = upper_bound_u64(X_VD, n_x, vd), cx = px >> 5;
 				int32_t below = n_kx;
 				if (cx < n_chunks) {
 					const uint64_t info = chunk[cx];
 					below = (int32_t)(info >> 32) + __popc((uint32_t)info & ((1u << (px & 31)) - 1));
 				}
-				a_vd[j + below] = vd, a_k[j + below] = ba_k[j];
+				A_VD[j + below] = vd, A_K[j + below] = BA_K[j];
 			}
 			n_new = n_kx + n_b;
 			__syncwarp();
@@ -579,6 +602,24 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 		if (p.w_out) p.w_out[r] = W;
 	}
 }
+#undef A_VD
+#undef X_VD
+#undef BA_VD
+#undef E_VD
+#undef F_VD
+#undef N_VD
+#undef TB
+#undef TA
+#undef ILO
+#undef IHI
+#undef CLO
+#undef CHI
+#undef A_K
+#undef X_K
+#undef BA_K
+#undef E_K
+#undef F_K
+#undef N_K
 
 // Plain form: one warp per queue position, arena offsets per read (main.cu:151-236 layout).
 __global__ void __launch_bounds__(256, 3) k_align_plain(const __grid_constant__ KParams p)
