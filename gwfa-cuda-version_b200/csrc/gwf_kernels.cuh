@@ -431,13 +431,28 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 		// ---- phase 4: ended-diagonal intervals, then the next wavefront
 		// (gwf_dedup / gwf_intv_merge2 / gwf_diag_dedup / gwf_mixed_dedup, gwf-ed.cu:780-804)
 		if (n_tb + n_ta > 0) {
-			warp_bitonic_sort(TA, nullptr, n_ta);
-			// rank-merge the old ranges with both point lists, ties ordered I < TB < TA
 			const int32_t n_c = n_i + n_tb + n_ta;
 			if (n_c > c.iv + c.tb + c.ta) {
 				st = ST_CAPACITY;
 				break;
 			}
+			if (n_c <= 32) {
+				// few ranges: one per lane, ordered by rank of the lower end (the union that the
+				// coalescing below computes does not depend on the order of equal ends)
+				uint64_t lo = PAD_KEY, hi = 0;
+				if (lane < n_i) lo = ILO[lane], hi = IHI[lane];
+				else if (lane < n_i + n_tb) lo = TB[lane - n_i], hi = lo + 1;
+				else if (lane < n_c) lo = TA[lane - n_i - n_tb], hi = lo + 1;
+				int32_t rank = 0;
+				for (int32_t t = 0; t < n_c; ++t) {
+					const uint64_t o2 = __shfl_sync(FULL, lo, t);
+					rank += o2 < lo || (o2 == lo && t < lane);
+				}
+				__syncwarp();
+				if (lane < n_c) CLO[rank] = lo, CHI[rank] = hi;
+			} else {
+			warp_bitonic_sort(TA, nullptr, n_ta);
+			// rank-merge the old ranges with both point lists, ties ordered I < TB < TA
 			for (int32_t j = lane; j < n_i; j += 32) {
 				const uint64_t x = ILO[j];
 				const int32_t pos = j + lower_bound_u64(TB, n_tb, x) + lower_bound_u64(TA, n_ta, x);
@@ -452,6 +467,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				const uint64_t x = TA[j];
 				const int32_t pos = j + upper_bound_u64(ILO, n_i, x) + upper_bound_u64(TB, n_tb, x);
 				CLO[pos] = x, CHI[pos] = x + 1;
+			}
 			}
 			__syncwarp();
 			// coalesce overlapping or touching ranges (gwf_intv_merge_adj, gwf-ed.cu:266-296)
