@@ -587,12 +587,21 @@ gwf_graph_t *load(LineSource &src, const char *start_seg)
 	}
 	uint32_t v0 = 0;
 	if (start_seg) {
-		auto it = gfa.names.find(start_seg);
+		// "name", or "name+" / "name-" for a strand: the reference starts on the forward strand
+		// only (main.cu:404 leaves the orientation as a TODO)
+		uint32_t strand = 0;
+		std::string name(start_seg);
+		auto it = gfa.names.find(name);
+		if (it == gfa.names.end() && name.size() > 1 && (name.back() == '+' || name.back() == '-')) {
+			strand = name.back() == '-' ? 1 : 0;
+			name.pop_back();
+			it = gfa.names.find(name);
+		}
 		if (it == gfa.names.end()) {
 			gwf_set_error("start segment not found");
 			return nullptr;
 		}
-		v0 = it->second << 1;
+		v0 = it->second << 1 | strand;
 	}
 	return to_gwf(gfa, v0);
 }

@@ -5,7 +5,7 @@
 //   gwf-b200 [-p] [-s STR] [-l INT] [-m persistent|plain] [-x] <target.gfa> <query.fa|fq[.gz]>
 //
 //   -p   print the graph (gwf_graph_print format) and exit     (main.cu:382-387, 354-359)
-//   -s   starting segment name [first]                          (main.cu:399-407)
+//   -s   starting segment name [first]; a trailing + or - picks the strand (main.cu:399-407)
 //   -l   max lag; accepted and ignored, as in the reference     (main.cu:371, 377)
 //   -m   execution form [persistent]
 //   -x   exact start state (GWF_F_EXACT_START)
@@ -72,7 +72,7 @@ void usage()
 	fprintf(stderr, "Usage: gwf-b200 [options] <target.gfa> <query.fa>\n");
 	fprintf(stderr, "Options:\n");
 	fprintf(stderr, "  -l INT    max lag behind the furthest wavefront; accepted and ignored [0]\n");
-	fprintf(stderr, "  -s STR    starting segment name [first]\n");
+	fprintf(stderr, "  -s STR    starting segment name, + or - appended for the strand [first, +]\n");
 	fprintf(stderr, "  -p        output GFA in the forward strand\n");
 	fprintf(stderr, "  -m STR    execution form: persistent or plain [persistent]\n");
 	fprintf(stderr, "  -x        exact start state (no reference start-state rule)\n");

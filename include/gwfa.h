@@ -200,8 +200,10 @@ void gwf_srv_destroy(gwf_srv_t *s);
 
 /* ---- GFA input side (reference gfa-io.c, gfa-base.c, gfa-sub.c, main.cu:294-359) ---- */
 
-/* gfa_read + gfa_finalize + gwf_gfa2gwf in one call. start_seg = segment name of v0, forward
- * strand (main.cu:399-407); NULL = first segment. Returns NULL on failure. */
+/* gfa_read + gfa_finalize + gwf_gfa2gwf in one call. start_seg = segment name of v0 on the
+ * forward strand (main.cu:399-407), or the name followed by '+' or '-' to choose the strand
+ * (the reference leaves that as a TODO, main.cu:404); NULL = first segment, forward. Vertex 0
+ * of the result is the start segment on that strand. Returns NULL on failure. */
 gwf_graph_t *gwf_gfa_load(const char *path, const char *start_seg);
 /* Same from an in-memory GFA text. */
 gwf_graph_t *gwf_gfa_load_mem(const char *text, int64_t len, const char *start_seg);

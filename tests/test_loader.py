@@ -38,6 +38,15 @@ def test_start_segment_and_orientation(G):
     assert g.arcs() == [(0, 1, 0)]
     with pytest.raises(G.GwfError):
         G.Graph.from_gfa_text(gfa, start_seg="zz")
+    # a strand suffix picks the start strand: "b+" is the default, "c+" walks c+ -> b- -> a-
+    assert G.Graph.from_gfa_text(gfa, start_seg="b+").seqs() == g.seqs()
+    gc = G.Graph.from_gfa_text(gfa, start_seg="c+")
+    assert gc.seqs() == [b"TTA", b"ACC", b"GTTT"] and gc.arcs() == [(0, 1, 0), (1, 2, 0)]
+    gb = G.Graph.from_gfa_text(gfa, start_seg="b-")
+    assert gb.seqs() == [b"ACC", b"GTTT"] and gb.arcs() == [(0, 1, 0)]
+    assert G.Graph.from_gfa_text(gfa, start_seg="c-").seqs() == [b"TAA"]
+    with pytest.raises(G.GwfError):
+        G.Graph.from_gfa_text(gfa, start_seg="zz-")
 
 
 def test_overlap_cigar_and_missing_overlap(G):
