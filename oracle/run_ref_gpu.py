@@ -6,6 +6,7 @@ Reads that the oracle flags as unsafe for the reference (arena overflow, non-ter
 left out so the reference is never given an input that can fault or hang; the count is reported.
 
     python oracle/run_ref_gpu.py config2 [config1 config3 config4] > gpurun_out/ref_gpu.json
+    python oracle/run_ref_gpu.py config4:2000      # the first 2,000 reads of a workload
 """
 import importlib.util
 import json
@@ -36,8 +37,9 @@ def main():
     G = pkg()
     harness = os.path.join(ROOT, "oracle", "_ref", "gwf-ref-harness")
     out = []
-    for kind in sys.argv[1:] or ["config2"]:
-        w = G.load_workload(kind)
+    for arg in sys.argv[1:] or ["config2"]:
+        kind, _, n = arg.partition(":")
+        w = G.load_workload(kind, n=int(n) if n else None)
         og = O.OracleGraph.from_graph(w["graph"])
         t0 = time.perf_counter()
         d_or, st, threads = og.ed_batch(w["cat"], w["offs"], w["lens"], w["v0"])
@@ -57,7 +59,7 @@ def main():
             raise SystemExit(kind + ": harness failed: " + res.stderr[-2000:])
         timing = json.loads(res.stderr.strip().splitlines()[-1])
         d_ref = np.array([int(x) for x in res.stdout.split()])
-        line = {"workload": kind, "reads": int(len(w["lens"])), "reads_run": int(len(keep)),
+        line = {"workload": arg, "reads": int(len(w["lens"])), "reads_run": int(len(keep)),
                 "reference_gpu_seconds": timing["seconds"], "reference_gpu_reads_per_s": timing["reads_per_s"],
                 "reference_launches": timing["launches"], "reference_streams": timing["streams"],
                 "oracle_threads": threads, "oracle_seconds": t_or,
