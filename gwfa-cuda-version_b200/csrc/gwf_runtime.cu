@@ -262,7 +262,9 @@ Engine::~Engine()
 	cudaSetDevice(device);
 	for (DBuf *b : {&pk_off, &order, &head, &retry_list, &retry_n, &ws, &slot_off, &w_out})
 		b->release();
-	for (HBuf *b : {&h_small}) b->release();
+	for (HBuf *b : {&h_small, &h_stage}) b->release();
+	for (cudaEvent_t e : stage_ev)
+		if (e) cudaEventDestroy(e);
 	if (stream) cudaStreamDestroy(stream);
 	if (ev0) cudaEventDestroy(ev0);
 	if (ev1) cudaEventDestroy(ev1);
@@ -280,7 +282,9 @@ Engine *gwf_engine(int dev)
 	E->device = dev;
 	cudaSetDevice(dev);
 	if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess ||
-	    cudaEventCreate(&E->ev0) != cudaSuccess || cudaEventCreate(&E->ev1) != cudaSuccess) {
+	    cudaEventCreate(&E->ev0) != cudaSuccess || cudaEventCreate(&E->ev1) != cudaSuccess ||
+	    cudaEventCreateWithFlags(&E->stage_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+	    cudaEventCreateWithFlags(&E->stage_ev[1], cudaEventDisableTiming) != cudaSuccess) {
 		cudaGetLastError();
 		gwf_set_error("stream/event creation failed");
 		delete E;
@@ -304,11 +308,38 @@ void Batch::release()
 {
 	for (DBuf *b : {&raw, &raw_off, &ql, &v0, &pk, &pk_off, &pure, &dist, &status, &steps, &order_ql})
 		b->release();
+	h_meta.release();
 	if (gexec) cudaGraphExecDestroy(gexec), gexec = nullptr;
 }
 
 // Copies n reads (host, concatenated) into the batch's device buffers; computes host-side
 // layout (packed offsets, cost order).
+// Host-to-device copy on the engine's stream. A page-locked source goes to the DMA engine as
+// it is; a pageable one of more than 1 MiB passes through two pinned 8 MiB chunks in turn, so
+// that filling one chunk overlaps the transfer of the other.
+static int upload(Engine &E, void *dst, const void *src, size_t n)
+{
+	cudaPointerAttributes at;
+	const bool pinned = cudaPointerGetAttributes(&at, src) == cudaSuccess && at.type == cudaMemoryTypeHost;
+	cudaGetLastError();
+	if (pinned || n <= ((size_t)1 << 20)) {
+		CK(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, E.stream));
+		return 0;
+	}
+	const size_t chunk = (size_t)8 << 20;
+	int rc;
+	if ((rc = E.h_stage.ensure(2 * chunk))) return rc;
+	for (size_t off = 0, i = 0; off < n; off += chunk, ++i) {
+		const size_t b = i & 1, len = std::min(chunk, n - off);
+		CK(cudaEventSynchronize(E.stage_ev[b])); // the DMA that last read this chunk, if any
+		char *stage = (char *)E.h_stage.p + b * chunk;
+		memcpy(stage, (const char *)src + off, len);
+		CK(cudaMemcpyAsync((char *)dst + off, stage, len, cudaMemcpyHostToDevice, E.stream));
+		CK(cudaEventRecord(E.stage_ev[b], E.stream));
+	}
+	return 0;
+}
+
 int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64_t *offs,
                    const int32_t *ql, const int32_t *v0, int32_t v1)
 {
@@ -324,11 +355,14 @@ int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64
 			hi = std::max(hi, offs[i] + ql[i]);
 		}
 	}
-	B.h_raw_off.resize((size_t)n);
-	for (int32_t i = 0; i < n; ++i) B.h_raw_off[(size_t)i] = offs[i] - lo;
-	B.h_pk_off.resize((size_t)n);
+	// pinned metadata: raw offsets and packed offsets (int64), queue order (int32)
+	int rc;
+	if ((rc = B.h_meta.ensure(20 * (size_t)n + 64))) return rc;
+	int64_t *h_raw_off = (int64_t *)B.h_meta.p, *h_pk_off = h_raw_off + n;
+	int32_t *h_order = (int32_t *)(h_pk_off + n);
+	for (int32_t i = 0; i < n; ++i) h_raw_off[i] = offs[i] - lo;
 	int64_t words = 0;
-	for (int32_t i = 0; i < n; ++i) B.h_pk_off[(size_t)i] = words, words += (ql[i] + 31) / 32 + 2;
+	for (int32_t i = 0; i < n; ++i) h_pk_off[i] = words, words += (ql[i] + 31) / 32 + 2;
 	B.pk_words = words;
 	// persistent queue: longest reads first (LPT scheduling on a cost ~ length estimate), as a
 	// counting sort over 64-base length buckets
@@ -344,11 +378,9 @@ int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64
 		std::vector<int32_t> cnt((size_t)nb + 1, 0);
 		for (int32_t i = 0; i < n; ++i) cnt[(size_t)(nb - 1 - (ql[i] >> 6)) + 1]++;
 		for (int32_t b = 0; b < nb; ++b) cnt[(size_t)b + 1] += cnt[(size_t)b];
-		B.h_order.resize((size_t)n);
-		for (int32_t i = 0; i < n; ++i) B.h_order[(size_t)cnt[(size_t)(nb - 1 - (ql[i] >> 6))]++] = i;
+		for (int32_t i = 0; i < n; ++i) h_order[cnt[(size_t)(nb - 1 - (ql[i] >> 6))]++] = i;
 	}
 	const size_t nraw = (size_t)(hi - lo) + 16;
-	int rc;
 	if ((rc = B.raw.ensure(nraw)) || (rc = B.raw_off.ensure(8 * (size_t)n + 8)) ||
 	    (rc = B.ql.ensure(4 * (size_t)n + 4)) || (rc = B.v0.ensure(4 * (size_t)n + 4)) ||
 	    (rc = B.pk.ensure(8 * (size_t)words + 8)) || (rc = B.pk_off.ensure(8 * (size_t)n + 8)) ||
@@ -358,13 +390,13 @@ int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64
 		return rc;
 	cudaStream_t s = E.stream;
 	if (n > 0) {
-		CK(cudaMemcpyAsync(B.raw.p, seqs + lo, (size_t)(hi - lo), cudaMemcpyHostToDevice, s));
+		if ((rc = upload(E, B.raw.p, seqs + lo, (size_t)(hi - lo)))) return rc;
 		CK(cudaMemsetAsync((char *)B.raw.p + (hi - lo), 0, 16, s));
-		CK(cudaMemcpyAsync(B.raw_off.p, B.h_raw_off.data(), 8 * (size_t)n, cudaMemcpyHostToDevice, s));
-		CK(cudaMemcpyAsync(B.ql.p, ql, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
-		CK(cudaMemcpyAsync(B.v0.p, v0, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
-		CK(cudaMemcpyAsync(B.pk_off.p, B.h_pk_off.data(), 8 * (size_t)n, cudaMemcpyHostToDevice, s));
-		CK(cudaMemcpyAsync(B.order_ql.p, B.h_order.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+		CK(cudaMemcpyAsync(B.raw_off.p, h_raw_off, 8 * (size_t)n, cudaMemcpyHostToDevice, s));
+		if ((rc = upload(E, B.ql.p, ql, 4 * (size_t)n)) || (rc = upload(E, B.v0.p, v0, 4 * (size_t)n)))
+			return rc;
+		CK(cudaMemcpyAsync(B.pk_off.p, h_pk_off, 8 * (size_t)n, cudaMemcpyHostToDevice, s));
+		CK(cudaMemcpyAsync(B.order_ql.p, h_order, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
 	}
 	return 0;
 }
@@ -620,9 +652,15 @@ int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t
 int gwf_batch_fetch(Engine &E, Batch &B, int32_t *dist, int32_t *status)
 {
 	if (B.n == 0) return 0;
-	if (dist) CK(cudaMemcpyAsync(dist, B.dist.p, 4 * (size_t)B.n, cudaMemcpyDeviceToHost, E.stream));
-	if (status) CK(cudaMemcpyAsync(status, B.status.p, 4 * (size_t)B.n, cudaMemcpyDeviceToHost, E.stream));
+	// through the pinned metadata buffer (its upload has completed: the stream is in order)
+	int rc;
+	if ((rc = B.h_meta.ensure(8 * (size_t)B.n + 64))) return rc;
+	int32_t *hd = (int32_t *)B.h_meta.p, *hs = hd + B.n;
+	if (dist) CK(cudaMemcpyAsync(hd, B.dist.p, 4 * (size_t)B.n, cudaMemcpyDeviceToHost, E.stream));
+	if (status) CK(cudaMemcpyAsync(hs, B.status.p, 4 * (size_t)B.n, cudaMemcpyDeviceToHost, E.stream));
 	CK(cudaStreamSynchronize(E.stream));
+	if (dist) memcpy(dist, hd, 4 * (size_t)B.n);
+	if (status) memcpy(status, hs, 4 * (size_t)B.n);
 	return 0;
 }
 

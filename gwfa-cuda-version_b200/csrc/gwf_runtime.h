@@ -41,6 +41,8 @@ struct Engine { // per-device launch state: stream, events, warp arenas
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 	DBuf pk_off, order, head, retry_list, retry_n, ws, slot_off, w_out;
 	HBuf h_small;
+	HBuf h_stage;                              // two pinned chunks for pageable uploads
+	cudaEvent_t stage_ev[2] = {nullptr, nullptr};
 	~Engine();
 };
 
@@ -51,8 +53,8 @@ struct Batch { // reads resident on the device
 	int32_t dom_bucket = 0;           // length bucket with the largest sum of ql^2 (autotuner)
 	cudaGraphExec_t gexec = nullptr;  // captured level-0 sequence of the persistent form
 	uint64_t gkey[8] = {};
-	std::vector<int32_t> h_ql, h_order;
-	std::vector<int64_t> h_raw_off, h_pk_off;
+	std::vector<int32_t> h_ql;
+	HBuf h_meta; // pinned: raw offsets, packed offsets, queue order; results on the way back
 	DBuf raw, raw_off, ql, v0, pk, pk_off, pure, dist, status, steps, order_ql;
 	void release();
 };
