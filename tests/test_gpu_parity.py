@@ -117,6 +117,19 @@ def test_long_reads_dense_graph_and_retries(G, O):
     assert np.array_equal(d, od)
 
 
+def test_serving_reads_match_oracle(G, O):
+    """Config 5 shapes (reads of U[500, 20000] bp at U[1%, 10%] on the 5 Mbp graph), the longest
+    the benchmarks use, through both batch forms, against the oracle."""
+    w = G.load_workload("config5", n=16)
+    g = _indexed(G, w["graph"])
+    og = O.OracleGraph.from_graph(w["graph"])
+    od, _, _ = og.ed_batch(w["cat"], w["offs"], w["lens"], w["v0"], stats=False)
+    for mode in (G.MODE_PERSISTENT, G.MODE_PLAIN):
+        d, st = g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode)
+        assert (st == 0).all()
+        assert np.array_equal(d, od)
+
+
 def test_resident_batch_runs_are_repeatable(G):
     w = G.load_workload("config1", n=500)
     g = _indexed(G, w["graph"])
