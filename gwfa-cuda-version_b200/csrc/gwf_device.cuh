@@ -323,6 +323,98 @@ __device__ __forceinline__ bool in_ranges(const uint64_t *lo, const uint64_t *hi
 }
 
 // Warp bitonic sort of keys[0..n) with int payload; buffers hold pow2ceil(n) entries.
+// Stable LSD radix sort of n diagonals (vd keys, optional int32 values) by one warp, for long
+// lists. The keys are first mapped to a dense mixed-radix integer, (v - v_min) * span_d +
+// (d - d_min), which keeps their order and usually needs 20-30 bits, then sorted 8 bits per pass
+// with a 256-bin histogram in shared memory (hist: 256 words owned by this warp). Equal digits
+// keep their input order: lanes with the same digit are ranked with __match_any_sync. tmp_keys /
+// tmp_vals hold n entries; the result is left in keys / vals. Returns false (nothing done) when
+// the dense keys would need more than 48 bits.
+static __device__ __noinline__ bool warp_radix_sort(uint64_t *keys, int32_t *vals, int32_t n,
+                                                    uint64_t *tmp_keys, int32_t *tmp_vals, uint32_t *hist)
+{
+	const int lane = threadIdx.x & 31;
+	uint32_t vmin = 0xffffffffu, vmax = 0;
+	uint32_t dmin = 0xffffffffu, dmax = 0; // the low word, d + 2^30, is unsigned
+	for (int32_t i = lane; i < n; i += 32) {
+		const uint64_t k = keys[i];
+		const uint32_t v = (uint32_t)(k >> 32), d = (uint32_t)k;
+		vmin = v < vmin ? v : vmin, vmax = v > vmax ? v : vmax;
+		dmin = d < dmin ? d : dmin, dmax = d > dmax ? d : dmax;
+	}
+	vmin = __reduce_min_sync(FULL, vmin), vmax = __reduce_max_sync(FULL, vmax);
+	dmin = __reduce_min_sync(FULL, dmin), dmax = __reduce_max_sync(FULL, dmax);
+	const uint64_t span_d = (uint64_t)(dmax - dmin) + 1;
+	const uint32_t span_v = vmax - vmin;
+	if ((span_v ? 32 - __clz(span_v) : 0) + (64 - __clzll((long long)span_d)) > 48) return false;
+	const uint64_t top = (uint64_t)span_v * span_d + (dmax - dmin); // largest dense key, < 2^48
+	const int32_t bits = 64 - __clzll((long long)top);
+	const int32_t passes = bits > 0 ? (bits + 7) / 8 : 1;
+	uint64_t *src_k = keys, *dst_k = tmp_keys;
+	int32_t *src_v = vals, *dst_v = tmp_vals;
+	for (int32_t pass = 0; pass < passes; ++pass) {
+		const int32_t shift = 8 * pass;
+		for (int32_t b = lane; b < 256; b += 32) hist[b] = 0;
+		__syncwarp();
+		for (int32_t base = 0; base < n; base += 32) {
+			const int32_t i = base + lane;
+			const bool act = i < n;
+			uint32_t digit = 256 + lane; // distinct and out of range for idle lanes
+			if (act) {
+				const uint64_t k = src_k[i];
+				const uint64_t dk = (uint64_t)((uint32_t)(k >> 32) - vmin) * span_d + ((uint32_t)k - dmin);
+				digit = (uint32_t)(dk >> shift) & 255u;
+			}
+			const uint32_t same = __match_any_sync(FULL, digit);
+			if (act && (same & lanemask_lt()) == 0) hist[digit] += __popc(same);
+			__syncwarp();
+		}
+		// exclusive scan of the 256 bins: 8 per lane, then across the warp
+		uint32_t c[8], sum = 0;
+#pragma unroll
+		for (int t = 0; t < 8; ++t) c[t] = hist[lane * 8 + t], sum += c[t];
+		int32_t tot;
+		uint32_t run = (uint32_t)warp_excl_scan((int32_t)sum, &tot);
+#pragma unroll
+		for (int t = 0; t < 8; ++t) hist[lane * 8 + t] = run, run += c[t];
+		__syncwarp();
+		for (int32_t base = 0; base < n; base += 32) {
+			const int32_t i = base + lane;
+			const bool act = i < n;
+			uint32_t digit = 256 + lane;
+			uint64_t k = 0;
+			int32_t v = 0;
+			if (act) {
+				k = src_k[i];
+				if (src_v) v = src_v[i];
+				const uint64_t dk = (uint64_t)((uint32_t)(k >> 32) - vmin) * span_d + ((uint32_t)k - dmin);
+				digit = (uint32_t)(dk >> shift) & 255u;
+			}
+			const uint32_t same = __match_any_sync(FULL, digit);
+			const uint32_t pos = act ? hist[digit] + __popc(same & lanemask_lt()) : 0;
+			__syncwarp();
+			if (act) {
+				dst_k[pos] = k;
+				if (src_v) dst_v[pos] = v;
+				if ((same & lanemask_lt()) == 0) hist[digit] += __popc(same);
+			}
+			__syncwarp();
+		}
+		uint64_t *tk = src_k;
+		src_k = dst_k, dst_k = tk;
+		int32_t *tv = src_v;
+		src_v = src_v ? dst_v : nullptr, dst_v = tv;
+	}
+	if (src_k != keys) { // an odd number of passes: copy back
+		for (int32_t i = lane; i < n; i += 32) {
+			keys[i] = src_k[i];
+			if (vals) vals[i] = src_v[i];
+		}
+	}
+	__syncwarp();
+	return true;
+}
+
 // Bitonic network in global memory for lists longer than 32 (kept out of line: it is rare).
 static __device__ __noinline__ void warp_bitonic_sort_global(uint64_t *keys, int32_t *vals, int32_t n)
 {

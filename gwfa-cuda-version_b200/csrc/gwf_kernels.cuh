@@ -81,12 +81,16 @@ __host__ __device__ inline int64_t srv_qbytes(int32_t ql)
 
 #ifndef GWF_KERNELS_DECL_ONLY
 // Aligns read r with one warp. All control flow is warp-uniform.
+// Candidate lists longer than this are radix-sorted; shorter ones by rank or a bitonic network.
+constexpr int32_t kRadixMin = 128;
+
 // The arena capacities are those of caps_for(min(ql, ql_cap), level): the arena at wsb must hold
 // them (callers size it for ql_cap, or for the read itself).
 __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *wsb, int32_t ql_cap, int32_t level)
 {
 	const int lane = threadIdx.x & 31;
 	const Caps c = caps_for(p.r.ql[r] < ql_cap ? p.r.ql[r] : ql_cap, level, p.dens_milli);
+
 	const DevGraph &g = p.g;
 	const WsOff o = ws_layout(c);
 	uint64_t *const h = (uint64_t *)(wsb + o.h);
@@ -128,6 +132,8 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 #define E_K ((int32_t *)(wsb + off_e_k))
 #define F_K ((int32_t *)(wsb + off_f_k))
 #define N_K ((int32_t *)(wsb + off_n_k))
+	// radix-sort histogram (256 bins): the interval scratch, free whenever a sort runs
+	uint32_t *const radix_hist = (uint32_t *)(wsb + off_clo);
 
 
 	ReadCtx rc;
@@ -451,7 +457,8 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				__syncwarp();
 				if (lane < n_c) CLO[rank] = lo, CHI[rank] = hi;
 			} else {
-			warp_bitonic_sort(TA, nullptr, n_ta);
+			if (n_ta <= kRadixMin || !warp_radix_sort(TA, nullptr, n_ta, A_VD, A_K, radix_hist))
+				warp_bitonic_sort(TA, nullptr, n_ta);
 			// rank-merge the old ranges with both point lists, ties ordered I < TB < TA
 			for (int32_t j = lane; j < n_i; j += 32) {
 				const uint64_t x = ILO[j];
@@ -527,7 +534,9 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 			off_a_vd = off_x_vd, off_a_k = off_x_k, off_x_vd = tv, off_x_k = tk;
 			__syncwarp();
 		} else {
-			warp_bitonic_sort(BA_VD, BA_K, n_ba);
+			// the wavefront buffer a is free until this step's merge writes it: sort scratch
+			if (n_ba <= kRadixMin || !warp_radix_sort(BA_VD, BA_K, n_ba, A_VD, A_K, radix_hist))
+				warp_bitonic_sort(BA_VD, BA_K, n_ba);
 			// 1. arc-side candidates: one per diagonal with the furthest k, minus those inside an
 			// ended interval; a diagonal also present among the in-vertex candidates folds its k
 			// into that entry (each in-vertex entry receives at most one, as the list is unique)
