@@ -322,11 +322,10 @@ __device__ __forceinline__ bool in_ranges(const uint64_t *lo, const uint64_t *hi
 	return j >= 0 && vd < hi[j];
 }
 
-// Warp bitonic sort of keys[0..n) with int payload; buffers hold pow2ceil(n) entries.
 // Stable LSD radix sort of n diagonals (vd keys, optional int32 values) by one warp, for long
 // lists. The keys are first mapped to a dense mixed-radix integer, (v - v_min) * span_d +
 // (d - d_min), which keeps their order and usually needs 20-30 bits, then sorted 8 bits per pass
-// with a 256-bin histogram in shared memory (hist: 256 words owned by this warp). Equal digits
+// with a 256-bin histogram (hist: 256 words of scratch owned by this warp). Equal digits
 // keep their input order: lanes with the same digit are ranked with __match_any_sync. tmp_keys /
 // tmp_vals hold n entries; the result is left in keys / vals. Returns false (nothing done) when
 // the dense keys would need more than 48 bits.
@@ -415,7 +414,8 @@ static __device__ __noinline__ bool warp_radix_sort(uint64_t *keys, int32_t *val
 	return true;
 }
 
-// Bitonic network in global memory for lists longer than 32 (kept out of line: it is rare).
+// Warp bitonic sort of keys[0..n) with int payload in global memory; buffers hold pow2ceil(n)
+// entries. For lists longer than 32 (kept out of line).
 static __device__ __noinline__ void warp_bitonic_sort_global(uint64_t *keys, int32_t *vals, int32_t n)
 {
 	const int lane = threadIdx.x & 31;
