@@ -150,3 +150,27 @@ def test_poll_and_unknown_request(G):
             srv.wait(10_000, 1, timeout_s=0.1)
     finally:
         srv.close()
+
+
+def test_failures_come_back_as_statuses(G):
+    """Host-side fault cases: an arena budget too small for a long read completes that read
+    with GWF_E_CAPACITY and still serves the short ones; a budget the device cannot hold makes
+    creation fail with an error, not a fault."""
+    w = G.load_workload("config3", n=200)
+    g = w["graph"]
+    g.index()
+    long_i = int(np.argmax(w["lens"]))
+    short = [i for i in range(len(w["lens"])) if w["lens"][i] < 1000][:6]
+    idx = np.array(short + [long_i])
+    reads, v0 = _subset(w, idx)
+    srv = G.Server(g, arena_budget_bytes=2 << 20)  # holds a few arenas of short reads only
+    try:
+        rid, k = srv.submit(reads, v0)
+        d, st = srv.wait(rid, k, timeout_s=120)
+    finally:
+        srv.close()
+    assert st[-1] == G.GWF_E_CAPACITY and d[-1] == -1
+    solo, st2 = g.ed_batch((reads[0], reads[1][:-1], reads[2][:-1]), v0[:-1])
+    assert (st[:-1] == 0).all() and np.array_equal(d[:-1], solo)
+    with pytest.raises(G.GwfError):
+        G.Server(g, arena_budget_bytes=1 << 50)
