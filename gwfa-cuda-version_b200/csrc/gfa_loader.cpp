@@ -10,7 +10,8 @@
 //   subgraph order     gfa-sub.c:41-272 (Kahn's algorithm with an ordered queue keyed by
 //                      (in-degree left, distance, vertex) and the orphan / forced rules)
 //   conversion         main.cu:294-345 (gwf_gfa2gwf), dump main.cu:354-359
-// The containers are this file's own (std::vector, std::set, std::unordered_map).
+// The containers are this file's own (std::vector, std::set, std::unordered_map, and an
+// open-addressing table of segment names).
 #include <zlib.h>
 #include <algorithm>
 #include <climits>
@@ -20,6 +21,7 @@
 #include <cstring>
 #include <set>
 #include <string>
+#include <string_view>
 #include <unordered_map>
 #include <vector>
 
@@ -45,20 +47,59 @@ struct Arc {
 	uint32_t head() const { return (uint32_t)(v_lv >> 32); }
 };
 
+// Segment names -> ids: open addressing over ids + 1 (0 = empty), FNV-1a hash, load <= 1/2.
+struct NameTable {
+	std::vector<uint32_t> slot;
+	size_t n = 0;
+	static uint64_t hash(std::string_view k)
+	{
+		uint64_t h = 1469598103934665603ULL;
+		for (unsigned char c : k) h = (h ^ c) * 1099511628211ULL;
+		return h;
+	}
+	// id of name, or -1; when absent and add is set, inserts new_id
+	int64_t find(const std::vector<Seg> &seg, std::string_view k) const
+	{
+		if (slot.empty()) return -1;
+		const size_t mask = slot.size() - 1;
+		for (size_t i = (size_t)hash(k) & mask;; i = (i + 1) & mask) {
+			const uint32_t e = slot[i];
+			if (!e) return -1;
+			if (seg[e - 1].name == k) return e - 1;
+		}
+	}
+	void insert(const std::vector<Seg> &seg, uint32_t id)
+	{
+		if (2 * (n + 1) > slot.size()) {
+			std::vector<uint32_t> old;
+			old.swap(slot);
+			slot.assign(old.empty() ? 1024 : old.size() * 2, 0);
+			n = 0;
+			for (uint32_t e : old)
+				if (e) insert(seg, e - 1);
+		}
+		const size_t mask = slot.size() - 1;
+		size_t i = (size_t)hash(seg[id].name) & mask;
+		while (slot[i]) i = (i + 1) & mask;
+		slot[i] = id + 1, ++n;
+	}
+};
+
 struct Gfa {
 	std::vector<Seg> seg;
-	std::unordered_map<std::string, uint32_t> names;
+	NameTable names;
 	std::vector<Arc> arc;
 	std::vector<uint64_t> idx; // per vertex: first << 32 | n
 
-	uint32_t add_seg(const std::string &name)
+	int64_t find_seg(std::string_view name) const { return names.find(seg, name); }
+	uint32_t add_seg(std::string_view name)
 	{
-		auto it = names.find(name);
-		if (it != names.end()) return it->second;
+		const int64_t f = names.find(seg, name);
+		if (f >= 0) return (uint32_t)f;
 		uint32_t id = (uint32_t)seg.size();
 		seg.emplace_back();
-		seg.back().name = name;
-		names.emplace(name, id);
+		seg.back().name.assign(name.data(), name.size());
+		names.insert(seg, id);
 		return id;
 	}
 	uint32_t n_vtx() const { return (uint32_t)seg.size() << 1; }
@@ -75,8 +116,28 @@ struct Gfa {
 	}
 	void arc_sort()
 	{
-		std::stable_sort(arc.begin(), arc.end(),
-		                 [](const Arc &x, const Arc &y) { return x.v_lv < y.v_lv; });
+		// arcs without lengths yet (low word 0) sort by their head vertex alone: a stable counting
+		// sort over 2 * segments buckets; otherwise a stable comparison sort on the full key
+		bool heads_only = true;
+		uint32_t max_head = 0;
+		for (const Arc &a : arc) {
+			if ((uint32_t)a.v_lv) {
+				heads_only = false;
+				break;
+			}
+			max_head = std::max(max_head, a.head());
+		}
+		if (!heads_only || arc.size() < 64) {
+			std::stable_sort(arc.begin(), arc.end(),
+			                 [](const Arc &x, const Arc &y) { return x.v_lv < y.v_lv; });
+			return;
+		}
+		std::vector<uint32_t> start((size_t)max_head + 2, 0);
+		for (const Arc &a : arc) ++start[(size_t)a.head() + 1];
+		for (size_t i = 1; i < start.size(); ++i) start[i] += start[i - 1];
+		std::vector<Arc> out(arc.size());
+		for (const Arc &a : arc) out[start[a.head()]++] = a;
+		arc.swap(out);
 	}
 	void arc_index() // gfa-base.c:214-229
 	{
@@ -92,84 +153,82 @@ struct Gfa {
 };
 
 // ---------------------------------------------------------------- tag helpers
-// Finds "XY:T:value" among tab-separated optional fields; returns pointer to value or null.
-const char *find_tag(const std::vector<std::string> &tags, const char *key, char type)
+using Fields = std::vector<std::string_view>;
+
+// Finds "XY:T:value" among tab-separated optional fields; returns a pointer to value or null.
+// The value runs to the next tab or the end of the line, so strtol stops where it should.
+const char *find_tag(const Fields &f, size_t first, const char *key, char type)
 {
-	for (const auto &t : tags)
-		if (t.size() >= 5 && t[0] == key[0] && t[1] == key[1] && t[2] == ':' && t[3] == type &&
-		    t[4] == ':')
-			return t.c_str() + 5;
+	for (size_t i = first; i < f.size(); ++i) {
+		const std::string_view t = f[i];
+		if (t.size() >= 5 && t[2] == ':' && t[4] == ':' &&
+		    (t[3] == 'A' || t[3] == 'i' || t[3] == 'f' || t[3] == 'Z' || t[3] == 'B') && t[0] == key[0] &&
+		    t[1] == key[1] && t[3] == type)
+			return t.data() + 5;
+	}
 	return nullptr;
 }
 
-void split_tabs(const std::string &line, std::vector<std::string> &out)
+void split_tabs(std::string_view line, Fields &out)
 {
 	out.clear();
 	size_t st = 0;
 	for (size_t i = 0; i <= line.size(); ++i)
 		if (i == line.size() || line[i] == '\t') {
-			out.emplace_back(line, st, i - st);
+			out.emplace_back(line.data() + st, i - st);
 			st = i + 1;
 		}
 }
 
-bool is_tag(const std::string &t)
-{
-	return t.size() >= 5 && t[2] == ':' && t[4] == ':' &&
-	       (t[3] == 'A' || t[3] == 'i' || t[3] == 'f' || t[3] == 'Z' || t[3] == 'B');
-}
-
 // gfa-io.c:115-220
-int parse_S(Gfa &g, const std::string &line)
+int parse_S(Gfa &g, std::string_view line, Fields &f)
 {
-	std::vector<std::string> f;
 	split_tabs(line, f); // f[0] == "S"
 	if (f.size() < 3) return -1;
-	const std::string &name = f[1], &sq = f[2];
-	std::vector<std::string> tags;
-	for (size_t i = 3; i < f.size(); ++i)
-		if (is_tag(f[i])) tags.push_back(f[i]);
+	const std::string_view name = f[1], sq = f[2];
 	int32_t LN = -1;
-	if (const char *p = find_tag(tags, "LN", 'i')) LN = (int32_t)strtol(p, nullptr, 10);
-	bool has_seq = !(sq.size() > 0 && sq[0] == '*');
+	if (const char *p = find_tag(f, 3, "LN", 'i')) LN = (int32_t)strtol(p, nullptr, 10);
+	const bool has_seq = !(sq.size() > 0 && sq[0] == '*');
 	int32_t len = 0;
 	if (!has_seq) {
 		if (LN >= 0) len = LN;
 	} else
-		len = (int32_t)strlen(sq.c_str());
+		len = (int32_t)sq.size();
 	uint32_t sid = g.add_seg(name);
 	Seg &s = g.seg[sid];
 	s.len = len;
 	s.has_seq = has_seq;
-	s.seq = has_seq ? std::string(sq.c_str()) : std::string();
+	if (has_seq) s.seq.assign(sq.data(), sq.size());
+	else s.seq.clear();
 	return 0;
 }
 
 // gfa-io.c:222-324
-int parse_L(Gfa &g, const std::string &line)
+int parse_L(Gfa &g, std::string_view line, Fields &f)
 {
-	std::vector<std::string> f;
 	split_tabs(line, f);
 	if (f.size() < 5) return -1;
-	const std::string &segv = f[1], &segw = f[3];
+	const std::string_view segv = f[1], segw = f[3];
 	if (f[2].empty() || (f[2][0] != '+' && f[2][0] != '-')) return -2;
 	if (f[4].empty() || (f[4][0] != '+' && f[4][0] != '-')) return -2;
 	int oriv = f[2][0] != '+', oriw = f[4][0] != '+';
 	int32_t ov = 0, ow = 0;
-	std::vector<std::string> tags;
+	size_t tags_from = f.size();
 	if (f.size() >= 6) {
-		const char *q = f[5].c_str();
+		// the field ends at a tab or at the end of the line: strtol and isdigit stop there
+		const char *q = f[5].data();
+		const char *qe = q + f[5].size();
 		bool ok = false;
-		if (*q == '*') {
+		if (q < qe && *q == '*') {
 			ov = ow = 0, ok = true;
-		} else if (*q == ':') {
+		} else if (q < qe && *q == ':') {
 			ov = INT32_MAX;
-			ow = isdigit((unsigned char)q[1]) ? (int32_t)strtol(q + 1, nullptr, 10) : INT32_MAX;
+			ow = q + 1 < qe && isdigit((unsigned char)q[1]) ? (int32_t)strtol(q + 1, nullptr, 10) : INT32_MAX;
 			ok = true;
-		} else if (isdigit((unsigned char)*q)) {
+		} else if (q < qe && isdigit((unsigned char)*q)) {
 			char *r;
 			long first = strtol(q, &r, 10);
-			if (isupper((unsigned char)*r)) { // CIGAR
+			if (r < qe && isupper((unsigned char)*r)) { // CIGAR
 				ov = ow = 0;
 				const char *p = q;
 				do {
@@ -179,28 +238,27 @@ int parse_L(Gfa &g, const std::string &line)
 					if (*p == 'M' || *p == 'D' || *p == 'N') ov += (int32_t)l;
 					if (*p == 'M' || *p == 'I' || *p == 'S') ow += (int32_t)l;
 					++p;
-				} while (isdigit((unsigned char)*p));
+				} while (p < qe && isdigit((unsigned char)*p));
 				ok = true;
-			} else if (*r == ':') {
+			} else if (r < qe && *r == ':') {
 				ov = (int32_t)first;
-				ow = isdigit((unsigned char)r[1]) ? (int32_t)strtol(r + 1, nullptr, 10) : INT32_MAX;
+				ow = r + 1 < qe && isdigit((unsigned char)r[1]) ? (int32_t)strtol(r + 1, nullptr, 10) : INT32_MAX;
 				ok = true;
 			}
 		}
 		if (!ok) ov = ow = 0; // unparsable overlap: treated like a missing field (gfa-io.c:277)
-		for (size_t i = 6; i < f.size(); ++i)
-			if (is_tag(f[i])) tags.push_back(f[i]);
+		tags_from = 6;
 	}
 	uint32_t v = g.add_seg(segv) << 1 | (uint32_t)oriv;
 	uint32_t w = g.add_seg(segw) << 1 | (uint32_t)oriw;
 	g.add_arc(v, w, ov, ow, -1, false);
-	if (const char *p = find_tag(tags, "L1", 'i'))
+	if (const char *p = find_tag(f, tags_from, "L1", 'i'))
 		if (ov != INT32_MAX) {
 			int32_t l1 = (int32_t)strtol(p, nullptr, 10);
 			Seg &s = g.seg[v >> 1];
 			if (ov + l1 > s.len) s.len = ov + l1;
 		}
-	if (const char *p = find_tag(tags, "L2", 'i'))
+	if (const char *p = find_tag(f, tags_from, "L2", 'i'))
 		if (ow != INT32_MAX) {
 			int32_t l2 = (int32_t)strtol(p, nullptr, 10);
 			Seg &s = g.seg[w >> 1];
@@ -323,35 +381,36 @@ struct LineSource {
 	int64_t bpos = 0, blen = 0;
 	bool eof = false;
 
-	bool getc_(int &c)
-	{
-		if (mem) {
-			if (mem_pos >= mem_len) return false;
-			c = (unsigned char)mem[mem_pos++];
-			return true;
-		}
-		if (bpos >= blen) {
-			if (eof) return false;
-			if (buf.empty()) buf.resize(1 << 16);
-			int r = gzread(fp, buf.data(), (unsigned)buf.size());
-			if (r <= 0) {
-				eof = true;
-				return false;
-			}
-			blen = r, bpos = 0;
-		}
-		c = (unsigned char)buf[bpos++];
-		return true;
-	}
 	bool getline(std::string &s)
 	{
 		s.clear();
-		int c;
 		bool any = false;
-		while (getc_(c)) {
+		for (;;) {
+			const char *p, *e;
+			if (mem) {
+				if (mem_pos >= mem_len) break;
+				p = mem + mem_pos, e = mem + mem_len;
+			} else {
+				if (bpos >= blen) {
+					if (eof) break;
+					if (buf.empty()) buf.resize(1 << 16);
+					int r = gzread(fp, buf.data(), (unsigned)buf.size());
+					if (r <= 0) {
+						eof = true;
+						break;
+					}
+					blen = r, bpos = 0;
+				}
+				p = buf.data() + bpos, e = buf.data() + blen;
+			}
 			any = true;
-			if (c == '\n') break;
-			s.push_back((char)c);
+			const char *nl = (const char *)memchr(p, '\n', (size_t)(e - p));
+			const char *stop = nl ? nl : e;
+			s.append(p, (size_t)(stop - p));
+			const int64_t used = (int64_t)(stop - p) + (nl ? 1 : 0);
+			if (mem) mem_pos += used;
+			else bpos += used;
+			if (nl) break;
 		}
 		if (!s.empty() && s.back() == '\r') s.pop_back();
 		return any;
@@ -361,6 +420,7 @@ struct LineSource {
 bool read_gfa(LineSource &src, Gfa &g)
 {
 	std::string s, fa_seq;
+	Fields fields;
 	bool is_fa = false;
 	int64_t fa_seg = -1;
 	auto flush_fa = [&]() {
@@ -387,8 +447,8 @@ bool read_gfa(LineSource &src, Gfa &g)
 		if (is_fa) continue;
 		if (s.size() < 3 || s[1] != '\t') continue;
 		int ret = 0;
-		if (s[0] == 'S') ret = parse_S(g, s);
-		else if (s[0] == 'L') ret = parse_L(g, s);
+		if (s[0] == 'S') ret = parse_S(g, s, fields);
+		else if (s[0] == 'L') ret = parse_L(g, s, fields);
 		(void)ret; // the reference reports and skips invalid lines
 	}
 	if (is_fa) flush_fa();
@@ -591,17 +651,17 @@ gwf_graph_t *load(LineSource &src, const char *start_seg)
 		// only (main.cu:404 leaves the orientation as a TODO)
 		uint32_t strand = 0;
 		std::string name(start_seg);
-		auto it = gfa.names.find(name);
-		if (it == gfa.names.end() && name.size() > 1 && (name.back() == '+' || name.back() == '-')) {
+		int64_t sid = gfa.find_seg(name);
+		if (sid < 0 && name.size() > 1 && (name.back() == '+' || name.back() == '-')) {
 			strand = name.back() == '-' ? 1 : 0;
 			name.pop_back();
-			it = gfa.names.find(name);
+			sid = gfa.find_seg(name);
 		}
-		if (it == gfa.names.end()) {
+		if (sid < 0) {
 			gwf_set_error("start segment not found");
 			return nullptr;
 		}
-		v0 = it->second << 1 | strand;
+		v0 = (uint32_t)sid << 1 | strand;
 	}
 	return to_gwf(gfa, v0);
 }
@@ -641,23 +701,45 @@ extern "C" void gwf_graph_free(gwf_graph_t *g)
 	free(g);
 }
 
+namespace {
+void put_int(std::string &out, int64_t x)
+{
+	char tmp[24];
+	int n = 0;
+	const bool neg = x < 0;
+	uint64_t u = neg ? (uint64_t)(-(x + 1)) + 1 : (uint64_t)x;
+	do {
+		tmp[n++] = (char)('0' + u % 10);
+		u /= 10;
+	} while (u);
+	if (neg) out += '-';
+	while (n) out += tmp[--n];
+}
+} // namespace
+
 extern "C" int64_t gwf_graph_dump(const gwf_graph_t *g, char *buf, int64_t cap)
 {
 	std::string out;
-	char tmp[96];
+	size_t est = 0;
+	for (uint32_t i = 0; i < g->n_vtx; ++i) est += g->len[i] + 32;
+	out.reserve(est + (size_t)g->n_arc * 40);
 	for (uint32_t i = 0; i < g->n_vtx; ++i) {
 		out += "S\t";
-		snprintf(tmp, sizeof tmp, "%d", (int)i);
-		out += tmp;
+		put_int(out, (int)i);
 		out += '\t';
 		out += g->seq[i];
-		snprintf(tmp, sizeof tmp, "\tLN:i:%d\n", (int)g->len[i]);
-		out += tmp;
+		out += "\tLN:i:";
+		put_int(out, (int)g->len[i]);
+		out += '\n';
 	}
 	for (uint32_t i = 0; i < g->n_arc; ++i) {
-		snprintf(tmp, sizeof tmp, "L\t%d\t+\t%d\t+\t%dM\n", (int)(uint32_t)(g->arc[i].a >> 32),
-		         (int)(uint32_t)g->arc[i].a, g->arc[i].o);
-		out += tmp;
+		out += "L\t";
+		put_int(out, (int)(uint32_t)(g->arc[i].a >> 32));
+		out += "\t+\t";
+		put_int(out, (int)(uint32_t)g->arc[i].a);
+		out += "\t+\t";
+		put_int(out, g->arc[i].o);
+		out += "M\n";
 	}
 	if (buf && cap > 0) {
 		int64_t n = (int64_t)out.size() < cap ? (int64_t)out.size() : cap;
