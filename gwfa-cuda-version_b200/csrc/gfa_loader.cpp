@@ -10,8 +10,8 @@
 //   subgraph order     gfa-sub.c:41-272 (Kahn's algorithm with an ordered queue keyed by
 //                      (in-degree left, distance, vertex) and the orphan / forced rules)
 //   conversion         main.cu:294-345 (gwf_gfa2gwf), dump main.cu:354-359
-// The containers are this file's own (std::vector, std::set, std::unordered_map, and an
-// open-addressing table of segment names).
+// The containers are this file's own (std::vector, std::set, byte pools for names and sequences,
+// and an open-addressing table of segment names).
 #include <zlib.h>
 #include <algorithm>
 #include <climits>
@@ -22,7 +22,6 @@
 #include <set>
 #include <string>
 #include <string_view>
-#include <unordered_map>
 #include <vector>
 
 #include "../../include/gwfa.h"
@@ -30,78 +29,115 @@
 
 namespace {
 
+// Names and sequences live in two byte pools; a redefined segment (a second S line with the same
+// name) points at its new bytes and leaves the old ones unused.
 struct Seg {
-	std::string name;
+	uint64_t seq_off = 0;
+	uint32_t seq_len = 0;
 	int32_t len = 0;
 	bool has_seq = false;
-	std::string seq;
 	bool del = false;
 };
 
 struct Arc {
 	uint64_t v_lv = 0; // vertex << 32 | lv
+	uint64_t link_id = 0;
 	uint32_t w = 0;
 	int32_t ov = 0, ow = 0;
-	uint64_t link_id = 0;
 	bool del = false, comp = false;
 	uint32_t head() const { return (uint32_t)(v_lv >> 32); }
 };
 
-// Segment names -> ids: open addressing over ids + 1 (0 = empty), FNV-1a hash, load <= 1/2.
+// Segment names -> ids: open addressing, load <= 1/2. Each name is one pool entry (its id, its
+// length, its bytes); a slot holds the high 24 bits of the name's hash above the entry's offset
+// (0 = empty; the pool starts with a pad), so a probe reads one slot and, when the tags agree,
+// one pool entry.
 struct NameTable {
-	std::vector<uint32_t> slot;
+	std::vector<uint64_t> slot;
+	std::vector<char> pool = std::vector<char>(8, 0);
 	size_t n = 0;
+	static constexpr uint64_t kOffMask = (1ULL << 40) - 1;
 	static uint64_t hash(std::string_view k)
 	{
 		uint64_t h = 1469598103934665603ULL;
 		for (unsigned char c : k) h = (h ^ c) * 1099511628211ULL;
-		return h;
+		return h ^ h >> 29;
 	}
-	// id of name, or -1; when absent and add is set, inserts new_id
-	int64_t find(const std::vector<Seg> &seg, std::string_view k) const
+	static uint64_t tag(uint64_t h) { return h >> 40 << 40; }
+	uint32_t entry_id(uint64_t off) const
+	{
+		uint32_t id;
+		memcpy(&id, pool.data() + off, 4);
+		return id;
+	}
+	std::string_view entry_name(uint64_t off) const
+	{
+		uint32_t len;
+		memcpy(&len, pool.data() + off + 4, 4);
+		return std::string_view(pool.data() + off + 8, len);
+	}
+	int64_t find(std::string_view k, uint64_t h) const
 	{
 		if (slot.empty()) return -1;
 		const size_t mask = slot.size() - 1;
-		for (size_t i = (size_t)hash(k) & mask;; i = (i + 1) & mask) {
-			const uint32_t e = slot[i];
+		const uint64_t t = tag(h);
+		for (size_t i = (size_t)h & mask;; i = (i + 1) & mask) {
+			const uint64_t e = slot[i];
 			if (!e) return -1;
-			if (seg[e - 1].name == k) return e - 1;
+			if ((e & ~kOffMask) == t && entry_name(e & kOffMask) == k) return entry_id(e & kOffMask);
 		}
 	}
-	void insert(const std::vector<Seg> &seg, uint32_t id)
+	void place(uint64_t h, uint64_t off)
 	{
+		const size_t mask = slot.size() - 1;
+		size_t i = (size_t)h & mask;
+		while (slot[i]) i = (i + 1) & mask;
+		slot[i] = tag(h) | off;
+	}
+	// appends the name with the given id; the caller has checked that it is absent
+	void add(std::string_view k, uint64_t h, uint32_t id)
+	{
+		const uint64_t off = pool.size();
+		const uint32_t len = (uint32_t)k.size();
+		pool.resize(off + 8 + len);
+		memcpy(pool.data() + off, &id, 4);
+		memcpy(pool.data() + off + 4, &len, 4);
+		memcpy(pool.data() + off + 8, k.data(), len);
 		if (2 * (n + 1) > slot.size()) {
-			std::vector<uint32_t> old;
+			std::vector<uint64_t> old;
 			old.swap(slot);
 			slot.assign(old.empty() ? 1024 : old.size() * 2, 0);
-			n = 0;
-			for (uint32_t e : old)
-				if (e) insert(seg, e - 1);
+			for (uint64_t e : old)
+				if (e) place(hash(entry_name(e & kOffMask)), e & kOffMask);
 		}
-		const size_t mask = slot.size() - 1;
-		size_t i = (size_t)hash(seg[id].name) & mask;
-		while (slot[i]) i = (i + 1) & mask;
-		slot[i] = id + 1, ++n;
+		place(h, off), ++n;
 	}
 };
 
 struct Gfa {
 	std::vector<Seg> seg;
 	NameTable names;
+	std::vector<char> seq_pool;
 	std::vector<Arc> arc;
 	std::vector<uint64_t> idx; // per vertex: first << 32 | n
 
-	int64_t find_seg(std::string_view name) const { return names.find(seg, name); }
+	int64_t find_seg(std::string_view name) const { return names.find(name, NameTable::hash(name)); }
 	uint32_t add_seg(std::string_view name)
 	{
-		const int64_t f = names.find(seg, name);
+		const uint64_t h = NameTable::hash(name);
+		const int64_t f = names.find(name, h);
 		if (f >= 0) return (uint32_t)f;
-		uint32_t id = (uint32_t)seg.size();
+		const uint32_t id = (uint32_t)seg.size();
 		seg.emplace_back();
-		seg.back().name.assign(name.data(), name.size());
-		names.insert(seg, id);
+		names.add(name, h, id);
 		return id;
 	}
+	void set_seq(Seg &s, std::string_view sq)
+	{
+		s.seq_off = seq_pool.size(), s.seq_len = (uint32_t)sq.size();
+		seq_pool.insert(seq_pool.end(), sq.begin(), sq.end());
+	}
+	const char *seq(const Seg &s) const { return seq_pool.data() + s.seq_off; }
 	uint32_t n_vtx() const { return (uint32_t)seg.size() << 1; }
 	uint32_t arc_n(uint32_t v) const { return v < idx.size() ? (uint32_t)idx[v] : 0; }
 	uint32_t arc_off(uint32_t v) const { return v < idx.size() ? (uint32_t)(idx[v] >> 32) : 0; }
@@ -198,8 +234,8 @@ int parse_S(Gfa &g, std::string_view line, Fields &f)
 	Seg &s = g.seg[sid];
 	s.len = len;
 	s.has_seq = has_seq;
-	if (has_seq) s.seq.assign(sq.data(), sq.size());
-	else s.seq.clear();
+	if (has_seq) g.set_seq(s, sq);
+	else s.seq_len = 0;
 	return 0;
 }
 
@@ -307,6 +343,7 @@ void fix_symm_add(Gfa &g) // gfa-base.c:303-338
 {
 	uint32_t nvt = g.n_vtx();
 	size_t n0 = g.arc.size();
+	g.arc.reserve(2 * n0); // at most one complement per arc
 	for (uint32_t v = 0; v < nvt; ++v) {
 		uint32_t nv = g.arc_n(v), ofs = g.arc_off(v);
 		for (uint32_t i = 0; i < nv; ++i) {
@@ -346,11 +383,12 @@ void fix_arc_len(Gfa &g) // gfa-base.c:249-267
 
 void cleanup(Gfa &g) // gfa-base.c:340-371
 {
-	std::vector<Arc> keep;
-	keep.reserve(g.arc.size());
-	for (const auto &a : g.arc)
-		if (!a.del && !g.seg[a.head() >> 1].del && !g.seg[a.w >> 1].del) keep.push_back(a);
-	g.arc.swap(keep);
+	size_t n = 0;
+	for (size_t e = 0; e < g.arc.size(); ++e) {
+		const Arc &a = g.arc[e];
+		if (!a.del && !g.seg[a.head() >> 1].del && !g.seg[a.w >> 1].del) g.arc[n++] = a;
+	}
+	g.arc.resize(n);
 	bool sorted = true;
 	for (size_t e = 1; e < g.arc.size(); ++e)
 		if (g.arc[e - 1].v_lv > g.arc[e].v_lv) {
@@ -426,7 +464,8 @@ bool read_gfa(LineSource &src, Gfa &g)
 	auto flush_fa = [&]() {
 		if (fa_seg >= 0) {
 			Seg &sg = g.seg[(size_t)fa_seg];
-			sg.seq = fa_seq, sg.has_seq = true, sg.len = (int32_t)fa_seq.size();
+			g.set_seq(sg, fa_seq);
+			sg.has_seq = true, sg.len = (int32_t)fa_seq.size();
 		}
 	};
 	while (src.getline(s)) {
@@ -479,23 +518,24 @@ struct Sub {
 
 void sub_from(const Gfa &g, uint32_t v0, int32_t max_dist, Sub &sub)
 {
-	std::unordered_map<uint32_t, TNode *> h;
+	// one node per oriented vertex at most: nodes live in a vector indexed by vertex, `made` says
+	// which exist (the reference keeps them in a hash table keyed by vertex)
+	const uint32_t nvt = g.n_vtx();
+	std::vector<TNode> node(nvt);
+	std::vector<uint8_t> made(nvt, 0);
 	std::set<TNode *, TCmp> tree;
-	std::vector<TNode *> L, owned;
+	std::vector<TNode *> L;
 	int32_t orphan_inv = 0;
 	auto gen = [&](uint32_t v, uint32_t d) {
-		TNode *p = new TNode;
-		owned.push_back(p);
+		TNode *p = &node[v];
+		made[v] = 1;
 		p->v = v, p->in_tree = 1, p->forced = false;
 		p->xnd = 1ULL << 63 | (uint64_t)g.arc_n(v ^ 1) << 32 | d;
 		return p;
 	};
-	auto get = [&](uint32_t v) -> TNode * {
-		auto it = h.find(v);
-		return it == h.end() ? nullptr : it->second;
-	};
+	auto get = [&](uint32_t v) -> TNode * { return v < nvt && made[v] ? &node[v] : nullptr; };
+	if (v0 >= nvt) return;
 	TNode *p0 = gen(v0, 0);
-	h[v0] = p0;
 	tree.insert(p0);
 	while (!tree.empty()) {
 		TNode *q = nullptr;
@@ -545,7 +585,6 @@ void sub_from(const Gfa &g, uint32_t v0, int32_t max_dist, Sub &sub)
 			TNode *p = get(avi.w);
 			if (!p) {
 				p = gen(avi.w, (uint32_t)dt);
-				h[avi.w] = p;
 			} else {
 				if (!p->in_tree) continue;
 				tree.erase(p);
@@ -573,7 +612,6 @@ void sub_from(const Gfa &g, uint32_t v0, int32_t max_dist, Sub &sub)
 		sub.n[j] = (int32_t)(sub.a.size() - o0);
 		std::sort(sub.a.begin() + (long)o0, sub.a.end());
 	}
-	for (TNode *p : owned) delete p;
 }
 
 // IUPAC complement, upper and lower case; every other byte maps to itself (U -> A).
@@ -615,15 +653,18 @@ gwf_graph_t *to_gwf(const Gfa &gfa, uint32_t v0) // main.cu:294-345
 		g->len[i] = len;
 		g->src[i] = v;
 		g->seq[i] = (char *)malloc(len + 1);
-		if (!s.has_seq || s.seq.size() < len) bad = true;
-		for (uint32_t j = 0; j < len; ++j) {
-			unsigned char c;
-			if (v & 1) {
-				size_t p = (size_t)len - j - 1;
-				c = p < s.seq.size() ? comp_base((unsigned char)s.seq[p]) : 'N';
-			} else
-				c = j < s.seq.size() ? (unsigned char)s.seq[j] : 'N';
-			g->seq[i][j] = (char)c;
+		if (!s.has_seq || s.seq_len < len) bad = true;
+		const char *sq = gfa.seq(s);
+		const uint32_t have = s.seq_len < len ? s.seq_len : len;
+		char *out = g->seq[i];
+		if (v & 1) {
+			for (uint32_t j = 0; j < len; ++j) {
+				const size_t p = (size_t)len - j - 1;
+				out[j] = p < s.seq_len ? (char)comp_base((unsigned char)sq[p]) : 'N';
+			}
+		} else {
+			memcpy(out, sq, have);
+			memset(out + have, 'N', len - have);
 		}
 		g->seq[i][len] = 0;
 		for (int32_t l = 0; l < sub.n[i]; ++l) {
@@ -702,49 +743,81 @@ extern "C" void gwf_graph_free(gwf_graph_t *g)
 }
 
 namespace {
-void put_int(std::string &out, int64_t x)
+int n_digits(int64_t x)
+{
+	uint64_t u = x < 0 ? (uint64_t)(-(x + 1)) + 1 : (uint64_t)x;
+	int n = x < 0 ? 2 : 1;
+	while (u >= 10) u /= 10, ++n;
+	return n;
+}
+
+char *put_int(char *p, int64_t x)
 {
 	char tmp[24];
 	int n = 0;
-	const bool neg = x < 0;
-	uint64_t u = neg ? (uint64_t)(-(x + 1)) + 1 : (uint64_t)x;
+	uint64_t u = x < 0 ? (uint64_t)(-(x + 1)) + 1 : (uint64_t)x;
 	do {
 		tmp[n++] = (char)('0' + u % 10);
 		u /= 10;
 	} while (u);
-	if (neg) out += '-';
-	while (n) out += tmp[--n];
+	if (x < 0) *p++ = '-';
+	while (n) *p++ = tmp[--n];
+	return p;
+}
+
+char *put_str(char *p, const char *s, size_t n)
+{
+	memcpy(p, s, n);
+	return p + n;
+}
+
+// the gwf_graph_print text (main.cu:354-359): "S\t<i>\t<seq>\tLN:i:<len>" per vertex, then
+// "L\t<v>\t+\t<w>\t+\t<o>M" per arc
+int64_t dump_size(const gwf_graph_t *g)
+{
+	int64_t n = 0;
+	for (uint32_t i = 0; i < g->n_vtx; ++i)
+		n += 2 + n_digits((int)i) + 1 + (int64_t)strlen(g->seq[i]) + 6 + n_digits((int)g->len[i]) + 1;
+	for (uint32_t i = 0; i < g->n_arc; ++i)
+		n += 2 + n_digits((int)(uint32_t)(g->arc[i].a >> 32)) + 3 + n_digits((int)(uint32_t)g->arc[i].a) + 3 +
+		     n_digits(g->arc[i].o) + 2;
+	return n;
+}
+
+void dump_into(const gwf_graph_t *g, char *p)
+{
+	for (uint32_t i = 0; i < g->n_vtx; ++i) {
+		p = put_str(p, "S\t", 2);
+		p = put_int(p, (int)i);
+		*p++ = '\t';
+		p = put_str(p, g->seq[i], strlen(g->seq[i]));
+		p = put_str(p, "\tLN:i:", 6);
+		p = put_int(p, (int)g->len[i]);
+		*p++ = '\n';
+	}
+	for (uint32_t i = 0; i < g->n_arc; ++i) {
+		p = put_str(p, "L\t", 2);
+		p = put_int(p, (int)(uint32_t)(g->arc[i].a >> 32));
+		p = put_str(p, "\t+\t", 3);
+		p = put_int(p, (int)(uint32_t)g->arc[i].a);
+		p = put_str(p, "\t+\t", 3);
+		p = put_int(p, g->arc[i].o);
+		p = put_str(p, "M\n", 2);
+	}
 }
 } // namespace
 
 extern "C" int64_t gwf_graph_dump(const gwf_graph_t *g, char *buf, int64_t cap)
 {
-	std::string out;
-	size_t est = 0;
-	for (uint32_t i = 0; i < g->n_vtx; ++i) est += g->len[i] + 32;
-	out.reserve(est + (size_t)g->n_arc * 40);
-	for (uint32_t i = 0; i < g->n_vtx; ++i) {
-		out += "S\t";
-		put_int(out, (int)i);
-		out += '\t';
-		out += g->seq[i];
-		out += "\tLN:i:";
-		put_int(out, (int)g->len[i]);
-		out += '\n';
+	const int64_t n = dump_size(g);
+	if (!buf || cap <= 0) return n;
+	if (cap > n) {
+		dump_into(g, buf);
+		buf[n] = 0;
+	} else {
+		std::vector<char> tmp((size_t)n);
+		dump_into(g, tmp.data());
+		memcpy(buf, tmp.data(), (size_t)cap);
 	}
-	for (uint32_t i = 0; i < g->n_arc; ++i) {
-		out += "L\t";
-		put_int(out, (int)(uint32_t)(g->arc[i].a >> 32));
-		out += "\t+\t";
-		put_int(out, (int)(uint32_t)g->arc[i].a);
-		out += "\t+\t";
-		put_int(out, g->arc[i].o);
-		out += "M\n";
-	}
-	if (buf && cap > 0) {
-		int64_t n = (int64_t)out.size() < cap ? (int64_t)out.size() : cap;
-		memcpy(buf, out.data(), (size_t)n);
-		if (n < cap) buf[n] = 0;
-	}
-	return (int64_t)out.size();
+	return n;
 }

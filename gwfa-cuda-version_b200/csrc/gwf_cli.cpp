@@ -116,15 +116,9 @@ int main(int argc, char *argv[])
 		return 1;
 	}
 	if (print_graph) {
-		// one call with a buffer that certainly holds the dump (a second call only if it does not)
-		int64_t cap = 64 + (int64_t)g->n_arc * 48;
-		for (uint32_t v = 0; v < g->n_vtx; ++v) cap += (int64_t)g->len[v] + 40;
-		std::vector<char> text((size_t)cap + 1);
-		int64_t n = gwf_graph_dump(g, text.data(), cap + 1);
-		if (n > cap) {
-			text.resize((size_t)n + 1);
-			n = gwf_graph_dump(g, text.data(), n + 1);
-		}
+		const int64_t n = gwf_graph_dump(g, nullptr, 0);
+		std::vector<char> text((size_t)n + 1);
+		gwf_graph_dump(g, text.data(), n + 1);
 		fwrite(text.data(), 1, (size_t)n, stdout);
 		gwf_graph_free(g);
 		return 0;

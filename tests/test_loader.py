@@ -1,7 +1,10 @@
 """GFA loader parity: the product loader's gwf_graph_print dump equals the reference
 `gwf-test -p` output (tests/golden/*.ref_dump.txt, from the reference binary)."""
+import ctypes
 import os
+import subprocess
 
+import numpy as np
 import pytest
 
 from conftest import GOLD
@@ -58,3 +61,76 @@ def test_overlap_cigar_and_missing_overlap(G):
 def test_fasta_as_graph(G):
     g = G.Graph.from_gfa_text(b">x desc\nACGT\nAC\n>y\nTT\n")
     assert g.n_vtx == 1 and g.seqs() == [b"ACGTAC"]
+
+
+def test_truncated_dump_returns_full_length(G):
+    g = G.Graph.from_gfa(os.path.join(GOLD, "graph_1000.gfa"))
+    full = g.dump()
+    buf = ctypes.create_string_buffer(100)
+    n = G.lib().gwf_graph_dump(g.ptr, buf, 100)
+    assert n == len(full) and buf.raw[:100] == full[:100]
+
+
+REF_GWF_TEST = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "gwf-test")
+
+
+def _random_gfa(rng):
+    """Names of 1-24 characters, redefined segments, LN tags, lower case and N, links on both
+    strands with 0M / * / short M overlaps, links to segments that are never defined. (The
+    reference crashes on '*' sequences, so none are generated here.)"""
+    n = int(rng.integers(2, 60))
+    names = []
+    while len(names) < n:
+        k = int(rng.integers(1, 25))
+        nm = "".join(rng.choice(list("abcxyz0123456789_"), size=k))
+        if nm not in names:
+            names.append(nm)
+    lines, lens = [], {}
+    order = list(rng.permutation(n))
+    for i in order + list(rng.choice(n, size=int(rng.integers(0, 4)))):
+        L = int(rng.integers(1, 40))
+        seq = "".join(rng.choice(list("ACGTACGTACGTacgtN"), size=L))
+        lines.append("S\t%s\t%s" % (names[i], seq) + ("\tLN:i:%d" % L if rng.random() < 0.3 else ""))
+        lens[names[i]] = L
+    ghosts = ["ghost%d" % j for j in range(int(rng.integers(1, 3)))] if rng.random() < 0.2 else []
+    for _ in range(int(rng.integers(n, 3 * n))):
+        if rng.random() < 0.7:  # mostly forward along the S-line order: large reachable parts
+            x = int(rng.integers(n - 1))
+            a, b = names[order[x]], names[order[x + 1 + int(rng.integers(min(3, n - 1 - x)))]]
+        else:
+            a, b = names[int(rng.integers(n))], names[int(rng.integers(n))]
+        if ghosts and rng.random() < 0.05:
+            a = ghosts[0]
+        r = rng.random()
+        if r < 0.7:
+            ov = "0M"
+        elif r < 0.85:
+            ov = "*"
+        else:
+            m = min(lens.get(a, 1), lens.get(b, 1))
+            ov = "%dM" % int(rng.integers(0, m + 1))
+        lines.append("L\t%s\t%s\t%s\t%s\t%s" % (a, "+-"[rng.random() < 0.3], b, "+-"[rng.random() < 0.3], ov))
+    return ("\n".join(lines) + "\n").encode()
+
+
+@pytest.mark.skipif(not os.path.exists(REF_GWF_TEST), reason="reference gwf-test not built")
+def test_random_gfa_dumps_match_reference_binary(G, tmp_path):
+    """Random GFA texts through the reference's own loader (gwf-test -p, built from its sources) and
+    through the product loader: identical dumps."""
+    rng = np.random.default_rng(99)
+    checked = 0
+    for t in range(60):
+        text = _random_gfa(rng)
+        path = tmp_path / ("g%d.gfa" % t)
+        path.write_bytes(text)
+        ref = subprocess.run([REF_GWF_TEST, "-p", str(path)], capture_output=True, timeout=60)
+        if ref.returncode != 0:
+            # the reference crashes on links to undefined segments, and on subgraphs whose arc
+            # count changes between its traversal and its extraction (main.cu:338 assertion)
+            assert b"not defined on an S-line" in ref.stderr or b"unusual bubble chain" in ref.stderr
+            continue
+        if b"unusual bubble chain" in ref.stderr:
+            continue  # fewer arcs extracted than counted: the reference dumps uninitialised arcs
+        assert G.Graph.from_gfa(str(path)).dump() == ref.stdout, text.decode()
+        checked += ref.stdout.count(b"S\t") > 3
+    assert checked > 30
