@@ -74,6 +74,7 @@ SIGNATURES = {
     "gwf_ed": (I32, [P, PG, I32, ctypes.c_char_p, I32, I32, U32, I32]),
     "gwf_ed_batch": (ctypes.c_int, [PG, I32, P, P, P, I32, U32, P, P, P]),
     "gwf_ed_batch_concat": (ctypes.c_int, [PG, I32, P, P, P, P, I32, U32, P, P, P]),
+    "gwf_ed_batch_path": (ctypes.c_int, [PG, I32, P, P, P, P, I32, I32, I32, P, P, P, P, P, P]),
     "gwf_batch_create": (P, [PG, I32, P, P, P, P, I32, P]),
     "gwf_batch_run": (ctypes.c_int, [P, P, P]),
     "gwf_batch_results": (ctypes.c_int, [P, P, P]),
@@ -284,6 +285,26 @@ class Graph:
         if rc != 0:
             raise GwfError(rc, last_error())
         return dist, st
+
+    def ed_path(self, reads, v0, v1=-1, flags=0, max_nv=4096):
+        """Alignment with traceback (gwf_ed_batch_path). Returns (dist, status, end_off, paths),
+        paths[i] = (vertices, arcs): the first min(path_n, max_nv) path vertices from v0 and the
+        index in the indexed graph's arcs of the arc into each (-1 for the first)."""
+        cat, offs, lens = reads if isinstance(reads, tuple) else pack_reads(reads)
+        n = len(lens)
+        v0 = np.ascontiguousarray(np.broadcast_to(np.asarray(v0, dtype=np.int32), (n,)))
+        dist = np.zeros(n, dtype=np.int32)
+        st = np.zeros(n, dtype=np.int32)
+        end_off = np.zeros(n, dtype=np.int32)
+        path_n = np.zeros(n, dtype=np.int32)
+        pv = np.zeros((max(n, 1), max(max_nv, 1)), dtype=np.int32)
+        pa = np.zeros((max(n, 1), max(max_nv, 1)), dtype=np.int32)
+        rc = lib().gwf_ed_batch_path(self.ptr, n, _ptr(cat), _ptr(offs), _ptr(lens), _ptr(v0), v1, flags, max_nv,
+                                     _ptr(dist), _ptr(st), _ptr(end_off), _ptr(path_n), _ptr(pv), _ptr(pa))
+        if rc != 0:
+            raise GwfError(rc, last_error())
+        paths = [(pv[i, :min(path_n[i], max_nv)].copy(), pa[i, :min(path_n[i], max_nv)].copy()) for i in range(n)]
+        return dist, st, end_off, paths
 
 
 TUNE_BUCKET_MAX = (1500, 3000, 6000, 12000, None)  # upper ql bound (exclusive) per bucket

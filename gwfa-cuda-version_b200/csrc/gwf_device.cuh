@@ -145,6 +145,33 @@ __host__ __device__ inline WsOff ws_layout(const Caps &c)
 	return o;
 }
 
+// Traceback form only: the trace id (int32) beside every k array, the (k, trace) pairs of the
+// arc-side candidates while they are sorted by index, and the trace log. A log record is
+// (arc index, parent record): one per arc transition (a free-match entry, or the deletion and
+// mismatch pair into a vertex), record 0 is the start state. Parents precede their children.
+struct TrOff {
+	int64_t a_t, x_t, ba_t, bk, w0_t, w1_t, n_t, log, total;
+	int32_t log_cap;
+};
+
+__host__ __device__ inline TrOff tr_layout(const Caps &c, int64_t base)
+{
+	TrOff o;
+	int64_t p = base;
+	const int64_t na = (int64_t)c.x + c.ba;
+	o.log_cap = c.h + 4 * c.a; // absent arrivals stay below c.h; the rest are query-end deletions
+	o.log = p, p = al16(p + 8LL * o.log_cap);
+	o.bk = p, p = al16(p + 8LL * c.ba);
+	o.a_t = p, p = al16(p + 4 * na);
+	o.x_t = p, p = al16(p + 4 * na);
+	o.ba_t = p, p = al16(p + 4LL * c.ba);
+	o.w0_t = p, p = al16(p + 4LL * c.w);
+	o.w1_t = p, p = al16(p + 4LL * c.w);
+	o.n_t = p, p = al16(p + 4LL * c.w);
+	o.total = al16(p);
+	return o;
+}
+
 #ifdef __CUDACC__
 
 __device__ __forceinline__ uint64_t gen_vd(uint32_t v, int32_t d)

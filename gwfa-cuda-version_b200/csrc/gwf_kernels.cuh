@@ -24,6 +24,12 @@ struct KParams {
 	int32_t *retry_n;
 	int32_t *steps_out;     // optional per-read score steps
 	int64_t *w_out;         // optional per-read sum of wavefront sizes
+	// traceback form only (per read r; the path rows are max_nv wide)
+	int32_t *end_off;       // offset in the last vertex of the last base consumed, -1 if none
+	int32_t *path_n;        // vertices on the path (only the first max_nv are written)
+	int32_t *path_v;        // path vertices from v0
+	int32_t *path_arc;      // arc index into path_v[j] (-1 for j = 0)
+	int32_t max_nv;
 };
 
 // ---- serving: one resident kernel, warps pull single reads from a device queue
@@ -85,8 +91,11 @@ __host__ __device__ inline int64_t srv_qbytes(int32_t ql)
 constexpr int32_t kRadixMin = 128;
 
 // The arena capacities are those of caps_for(min(ql, ql_cap), level): the arena at wsb must hold
-// them (callers size it for ql_cap, or for the read itself).
-__device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *wsb, int32_t ql_cap, int32_t level)
+// them (callers size it for ql_cap, or for the read itself). With TR, the arena also holds
+// tr_layout's arrays after ws_layout's, every state carries the id of the trace record of the
+// last arc it crossed, and the read's path is written to p.path_*.
+template <bool TR>
+__device__ __noinline__ void align_read_t(const KParams &p, int32_t r, uint8_t *wsb, int32_t ql_cap, int32_t level)
 {
 	const int lane = threadIdx.x & 31;
 	const Caps c = caps_for(p.r.ql[r] < ql_cap ? p.r.ql[r] : ql_cap, level, p.dens_milli);
@@ -114,6 +123,16 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 	uint32_t off_e_k = (uint32_t)o.w0_k;
 	uint32_t off_f_k = (uint32_t)o.w1_k;
 	const uint32_t off_n_k = (uint32_t)o.n_k;
+	// traceback arrays (dead code without TR)
+	const TrOff to = tr_layout(c, o.total);
+	uint32_t off_a_t = (uint32_t)to.a_t;
+	uint32_t off_x_t = (uint32_t)to.x_t;
+	const uint32_t off_ba_t = (uint32_t)to.ba_t;
+	uint32_t off_e_t = (uint32_t)to.w0_t;
+	uint32_t off_f_t = (uint32_t)to.w1_t;
+	const uint32_t off_n_t = (uint32_t)to.n_t;
+	const uint32_t off_bk = (uint32_t)to.bk;
+	const uint32_t off_log = (uint32_t)to.log;
 #define A_VD ((uint64_t *)(wsb + off_a_vd))
 #define X_VD ((uint64_t *)(wsb + off_x_vd))
 #define BA_VD ((uint64_t *)(wsb + off_ba_vd))
@@ -132,6 +151,14 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 #define E_K ((int32_t *)(wsb + off_e_k))
 #define F_K ((int32_t *)(wsb + off_f_k))
 #define N_K ((int32_t *)(wsb + off_n_k))
+#define A_T ((int32_t *)(wsb + off_a_t))
+#define X_T ((int32_t *)(wsb + off_x_t))
+#define BA_T ((int32_t *)(wsb + off_ba_t))
+#define E_T ((int32_t *)(wsb + off_e_t))
+#define F_T ((int32_t *)(wsb + off_f_t))
+#define N_T ((int32_t *)(wsb + off_n_t))
+#define BK ((int2 *)(wsb + off_bk))
+#define TLOG ((uint2 *)(wsb + off_log))
 	// radix-sort histogram (256 bins): the interval scratch, free whenever a sort runs
 	uint32_t *const radix_hist = (uint32_t *)(wsb + off_clo);
 
@@ -149,11 +176,17 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 	int32_t dist = -1, st = ST_OK, steps = 0;
 	int64_t W = 0;
 	if (ql <= 0 || v0 < 0 || (uint32_t)v0 >= g.n_vtx || (v1 >= 0 && (uint32_t)v1 >= g.n_vtx)) {
-		if (lane == 0) p.dist[r] = -1, p.status[r] = ST_BAD_INPUT;
+		if (lane == 0) {
+			p.dist[r] = -1, p.status[r] = ST_BAD_INPUT;
+			if constexpr (TR) p.path_n[r] = 0, p.end_off[r] = -1;
+		}
 		return;
 	}
-	if (o.total > 0xffffffffLL) { // the 32-bit offsets above (caps_for keeps arenas below 4 GB)
-		if (lane == 0) p.dist[r] = -1, p.status[r] = ST_CAPACITY;
+	if (o.total > 0xffffffffLL || (TR && to.total > 0xffffffffLL)) { // the 32-bit offsets above
+		if (lane == 0) {
+			p.dist[r] = -1, p.status[r] = ST_CAPACITY;
+			if constexpr (TR) p.path_n[r] = 0, p.end_off[r] = -1;
+		}
 		return;
 	}
 
@@ -164,6 +197,11 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 		for (int32_t i = lane; i < c.h / 2; i += 32) h4[i] = z;
 	}
 	if (lane == 0) A_VD[0] = gen_vd((uint32_t)v0, 0), A_K[0] = -1; // gwf-ed.cu:1303-1308
+	int32_t n_log = 1;                  // trace records in use
+	int32_t tr_t = -1, tr_k = -1;       // trace record and offset of the state that ends the read
+	if constexpr (TR) {
+		if (lane == 0) A_T[0] = 0, TLOG[0] = make_uint2(0xffffffffu, 0xffffffffu);
+	}
 	__syncwarp();
 	const uint32_t hmask = (uint32_t)c.h - 1;
 	const int32_t hlimit = c.h - c.h / 4;
@@ -178,6 +216,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 		++steps;
 		W += n_a;
 		bool found = false, ovf = false;
+		int32_t f_j = 0x7fffffff, f_t = -1, f_k = -1; // TR: this lane's first end state
 
 		// ---- phase 1: extend every diagonal; collect vertex-end (and, for v1 >= 0,
 		// query-end) states into the first wave (gwf-ed.cu:902-910, 965-984)
@@ -186,28 +225,40 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 			const int32_t j = base + lane;
 			bool toE = false;
 			uint64_t vd = 0;
-			int32_t k = 0;
+			int32_t k = 0, t = 0;
 			if (j < n_a) {
 				vd = A_VD[j];
 				k = A_K[j];
+				if constexpr (TR) t = A_T[j];
 				const uint32_t v = vd_v(vd);
 				const int32_t d = vd_d(vd), vl = (int32_t)__ldg(g.len + v);
 				k = ext(g, rc, v, d, k, vl);
 				A_K[j] = k;
 				const bool vend = k == vl - 1, qend = d + k == ql - 1;
 				if (qend) {
-					if (v1 < 0 || ((int32_t)v == v1 && vend)) found = true;
-					else toE = true;
+					if (v1 < 0 || ((int32_t)v == v1 && vend)) {
+						found = true;
+						if (TR && j < f_j) f_j = j, f_t = t, f_k = k;
+					} else
+						toE = true;
 				} else if (vend)
 					toE = true;
 			}
 			const uint32_t m = __ballot_sync(FULL, toE);
 			const int32_t pos = n_e + __popc(m & lanemask_lt());
-			if (toE && pos < c.w) E_VD[pos] = vd, E_K[pos] = k;
+			if (toE && pos < c.w) {
+				E_VD[pos] = vd, E_K[pos] = k;
+				if constexpr (TR) E_T[pos] = t;
+			}
 			n_e += __popc(m);
 		}
 		if (__any_sync(FULL, found)) {
 			dist = s;
+			if constexpr (TR) {
+				const int32_t mj = (int32_t)__reduce_min_sync(FULL, (uint32_t)f_j);
+				const int src = __ffs(__ballot_sync(FULL, f_j == mj)) - 1;
+				tr_t = __shfl_sync(FULL, f_t, src), tr_k = __shfl_sync(FULL, f_k, src);
+			}
 			break;
 		}
 		if (n_e > c.w) ovf = true;
@@ -219,11 +270,17 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 		for (int32_t base = 0; base < n_a; base += 32) {
 			const int32_t j = base + lane;
 			uint64_t cv[3];
-			int32_t ck[3];
+			int32_t ck[3], ct[3] = {0, 0, 0};
 			bool keep[3] = {false, false, false}, tmp[3] = {false, false, false};
 			if (j < n_a) {
 				const uint64_t vd = A_VD[j];
 				const int32_t k = A_K[j];
+				int32_t tt = 0, pt = 0, nt = 0;
+				if constexpr (TR) {
+					tt = A_T[j];
+					pt = j > 0 ? A_T[j - 1] : 0;
+					nt = j + 1 < n_a ? A_T[j + 1] : 0;
+				}
 				const int32_t vl = (int32_t)__ldg(g.len + vd_v(vd));
 				const uint64_t pv = j > 0 ? A_VD[j - 1] : 0;
 				const int32_t pk = j > 0 ? A_K[j - 1] : 0;
@@ -235,18 +292,18 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				// L: diagonal d-1 when absent from a: deletion from d, insertion from d-2
 				has[0] = !left_in;
 				cv[0] = vd - 1;
-				ck[0] = k + 1;
-				if (left2 && pk > ck[0]) ck[0] = pk;
+				ck[0] = k + 1, ct[0] = tt;
+				if (left2 && pk > ck[0]) ck[0] = pk, ct[0] = pt;
 				// S: diagonal d: mismatch, insertion from d-1, deletion from d+1
 				has[1] = true;
 				cv[1] = vd;
-				ck[1] = k + 1;
-				if (left_in && pk > ck[1]) ck[1] = pk;
-				if (right_in && nk + 1 > ck[1]) ck[1] = nk + 1;
+				ck[1] = k + 1, ct[1] = tt;
+				if (left_in && pk > ck[1]) ck[1] = pk, ct[1] = pt;
+				if (right_in && nk + 1 > ck[1]) ck[1] = nk + 1, ct[1] = nt;
 				// R: diagonal d+1 when neither d+1 nor d+2 is in a: insertion from d
 				has[2] = !right_in && !right2;
 				cv[2] = vd + 1;
-				ck[2] = k;
+				ck[2] = k, ct[2] = tt;
 				// the reference keeps vl in a uint32_t here (gwf-ed.cu:895, 993): a candidate
 				// with k = -1 (insertion before the first base of v0) fails `k < vl` and is dropped
 #pragma unroll
@@ -266,7 +323,10 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 #pragma unroll
 				for (int t = 0; t < 3; ++t)
 					if (keep[t]) {
-						if (off < c.x) X_VD[off] = cv[t], X_K[off] = ck[t];
+						if (off < c.x) {
+							X_VD[off] = cv[t], X_K[off] = ck[t];
+							if constexpr (TR) X_T[off] = ct[t];
+						}
 						++off;
 					}
 				n_x += __popc(k0) + __popc(k1) + __popc(k2);
@@ -300,10 +360,11 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				const int32_t j = base + lane;
 				bool act = j < n_e, isq = false, isv = false;
 				uint64_t vd = 0;
-				int32_t k = 0, d = 0, vl = 0, i = 0, nv = 0;
+				int32_t k = 0, d = 0, vl = 0, i = 0, nv = 0, et = 0;
 				uint32_t v = 0, aoff = 0;
 				if (act) {
 					vd = E_VD[j], k = E_K[j];
+					if constexpr (TR) et = E_T[j];
 					v = vd_v(vd), d = vd_d(vd), vl = (int32_t)__ldg(g.len + v), i = d + k;
 					isq = i == ql - 1;
 					isv = !isq;
@@ -340,9 +401,20 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 						} else
 							one = true; // v1 >= 0: query end at a vertex end, delete into w
 					}
+					int32_t rec = 0; // TR: the record of this arc transition
+					if constexpr (TR) {
+						const bool mk = enter || two || one;
+						const uint32_t mr = __ballot_sync(FULL, mk);
+						rec = n_log + __popc(mr & lanemask_lt());
+						if (mk && rec < to.log_cap) TLOG[rec] = make_uint2(aoff + (uint32_t)t, (uint32_t)et);
+						n_log += __popc(mr);
+					}
 					const uint32_t me = __ballot_sync(FULL, enter);
 					const int32_t pe = n_n + __popc(me & lanemask_lt());
-					if (enter && pe < c.w) N_VD[pe] = gen_vd(w, i + 1 - ol), N_K[pe] = ol;
+					if (enter && pe < c.w) {
+						N_VD[pe] = gen_vd(w, i + 1 - ol), N_K[pe] = ol;
+						if constexpr (TR) N_T[pe] = rec;
+					}
 					n_n += __popc(me);
 					int32_t tot;
 					int32_t pb = warp_excl_scan(two ? 2 : (one ? 1 : 0), &tot) + n_ba;
@@ -350,9 +422,13 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 						if (pb + 1 < c.ba) {
 							BA_VD[pb] = gen_vd(w, i - ol), BA_K[pb] = ol;         // deletion
 							BA_VD[pb + 1] = gen_vd(w, i + 1 - ol), BA_K[pb + 1] = ol; // mismatch
+							if constexpr (TR) BA_T[pb] = rec, BA_T[pb + 1] = rec;
 						}
 					} else if (one) {
-						if (pb < c.ba) BA_VD[pb] = gen_vd(w, i - ol), BA_K[pb] = ol;
+						if (pb < c.ba) {
+							BA_VD[pb] = gen_vd(w, i - ol), BA_K[pb] = ol;
+							if constexpr (TR) BA_T[pb] = rec;
+						}
 					}
 					n_ba += tot;
 				}
@@ -365,6 +441,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				if ((ins || qdel) && pi < c.ba) {
 					BA_VD[pi] = ins ? gen_vd(v, d + 1) : gen_vd(v, d - 1);
 					BA_K[pi] = ins ? k : k + 1;
+					if constexpr (TR) BA_T[pi] = et;
 				}
 				n_ba += __popc(mi);
 			}
@@ -374,6 +451,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				if (tot > hlimit) ovf = true;
 			}
 			if (n_n > c.w || n_ba > c.ba || n_ta > c.ta) ovf = true;
+			if (TR && n_log > to.log_cap) ovf = true;
 			if (__any_sync(FULL, ovf)) {
 				ovf = true;
 				break;
@@ -385,17 +463,21 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				const int32_t j = base + lane;
 				bool toF = false, three = false;
 				uint64_t vd = 0;
-				int32_t k = 0, d = 0;
+				int32_t k = 0, d = 0, nt = 0;
 				uint32_t v = 0;
 				if (j < n_n) {
 					vd = N_VD[j], k = N_K[j];
+					if constexpr (TR) nt = N_T[j];
 					v = vd_v(vd), d = vd_d(vd);
 					const int32_t vl = (int32_t)__ldg(g.len + v);
 					k = ext(g, rc, v, d, k, vl);
 					const int32_t i = d + k;
 					if (i == ql - 1) {
-						if (v1 < 0 || ((int32_t)v == v1 && k == vl - 1)) found = true;
-						else toF = true;
+						if (v1 < 0 || ((int32_t)v == v1 && k == vl - 1)) {
+							found = true;
+							if (TR && j < f_j) f_j = j, f_t = nt, f_k = k;
+						} else
+							toF = true;
 					} else if (k + 1 < vl)
 						three = true;
 					else
@@ -403,7 +485,10 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				}
 				const uint32_t mf = __ballot_sync(FULL, toF);
 				const int32_t pf = n_f + __popc(mf & lanemask_lt());
-				if (toF && pf < c.w) F_VD[pf] = vd, F_K[pf] = k;
+				if (toF && pf < c.w) {
+					F_VD[pf] = vd, F_K[pf] = k;
+					if constexpr (TR) F_T[pf] = nt;
+				}
 				n_f += __popc(mf);
 				const uint32_t m3 = __ballot_sync(FULL, three);
 				const int32_t p3 = n_ba + 3 * __popc(m3 & lanemask_lt());
@@ -411,6 +496,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 					BA_VD[p3] = gen_vd(v, d - 1), BA_K[p3] = k + 1;     // deletion
 					BA_VD[p3 + 1] = gen_vd(v, d), BA_K[p3 + 1] = k + 1; // mismatch
 					BA_VD[p3 + 2] = gen_vd(v, d + 1), BA_K[p3 + 2] = k; // insertion
+					if constexpr (TR) BA_T[p3] = nt, BA_T[p3 + 1] = nt, BA_T[p3 + 2] = nt;
 				}
 				n_ba += 3 * __popc(m3);
 			}
@@ -420,12 +506,18 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				break;
 			}
 			__syncwarp();
-			const uint32_t tv = off_e_vd, tk = off_e_k;
+			const uint32_t tv = off_e_vd, tk = off_e_k, tt = off_e_t;
 			off_e_vd = off_f_vd, off_e_k = off_f_k, off_f_vd = tv, off_f_k = tk;
+			off_e_t = off_f_t, off_f_t = tt;
 			n_e = n_f;
 		}
 		if (__any_sync(FULL, found)) {
 			dist = s;
+			if constexpr (TR) {
+				const int32_t mj = (int32_t)__reduce_min_sync(FULL, (uint32_t)f_j);
+				const int src = __ffs(__ballot_sync(FULL, f_j == mj)) - 1;
+				tr_t = __shfl_sync(FULL, f_t, src), tr_k = __shfl_sync(FULL, f_k, src);
+			}
 			break;
 		}
 		if (__any_sync(FULL, ovf)) {
@@ -517,23 +609,31 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 			for (int32_t base = 0; base < n_x; base += 32) {
 				const int32_t j = base + lane;
 				uint64_t vd = 0;
-				int32_t k = 0;
+				int32_t k = 0, t = 0;
 				bool keep = false;
 				if (j < n_x) {
 					vd = X_VD[j], k = X_K[j];
+					if constexpr (TR) t = X_T[j];
 					keep = !in_ranges(ILO, IHI, n_i, vd, i_min, i_max);
 				}
 				const uint32_t m = __ballot_sync(FULL, keep);
 				if (keep) {
 					const int32_t pos = n_new + __popc(m & lanemask_lt());
 					X_VD[pos] = vd, X_K[pos] = k;
+					if constexpr (TR) X_T[pos] = t;
 				}
 				n_new += __popc(m);
 			}
-			const uint32_t tv = off_a_vd, tk = off_a_k;
+			const uint32_t tv = off_a_vd, tk = off_a_k, tt = off_a_t;
 			off_a_vd = off_x_vd, off_a_k = off_x_k, off_x_vd = tv, off_x_k = tk;
+			off_a_t = off_x_t, off_x_t = tt;
 			__syncwarp();
 		} else {
+			// TR: the candidates' (k, trace) pairs move aside and the sort carries their indices
+			if constexpr (TR) {
+				for (int32_t j = lane; j < n_ba; j += 32) BK[j] = make_int2(BA_K[j], BA_T[j]), BA_K[j] = j;
+				__syncwarp();
+			}
 			// the wavefront buffer a is free until this step's merge writes it: sort scratch
 			if (n_ba <= kRadixMin || !warp_radix_sort(BA_VD, BA_K, n_ba, A_VD, A_K, radix_hist))
 				warp_bitonic_sort(BA_VD, BA_K, n_ba);
@@ -545,19 +645,31 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				const int32_t j = base + lane;
 				bool keep = false;
 				uint64_t vd = 0;
-				int32_t k = 0;
+				int32_t k = 0, tk = 0;
 				if (j < n_ba) {
 					vd = BA_VD[j], k = BA_K[j];
+					if constexpr (TR) {
+						const int2 e = BK[k];
+						k = e.x, tk = e.y;
+					}
 					if (j == 0 || BA_VD[j - 1] != vd) {
 						for (int32_t t = j + 1; t < n_ba && BA_VD[t] == vd; ++t) {
-							const int32_t kt = BA_K[t];
-							k = kt > k ? kt : k;
+							if constexpr (TR) {
+								const int2 e = BK[BA_K[t]];
+								if (e.x > k) k = e.x, tk = e.y;
+							} else {
+								const int32_t kt = BA_K[t];
+								k = kt > k ? kt : k;
+							}
 						}
 						keep = !in_ranges(ILO, IHI, n_i, vd, i_min, i_max);
 						if (keep) {
 							const int32_t px = upper_bound_u64(X_VD, n_x, vd);
 							if (px > 0 && X_VD[px - 1] == vd) {
-								if (k > X_K[px - 1]) X_K[px - 1] = k;
+								if (k > X_K[px - 1]) {
+									X_K[px - 1] = k;
+									if constexpr (TR) X_T[px - 1] = tk;
+								}
 								keep = false;
 							}
 						}
@@ -568,6 +680,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				if (keep) {
 					const int32_t pos = n_b + __popc(m & lanemask_lt());
 					BA_VD[pos] = vd, BA_K[pos] = k;
+					if constexpr (TR) BA_T[pos] = tk;
 				}
 				n_b += __popc(m);
 				__syncwarp();
@@ -580,9 +693,10 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				const int32_t j = base + lane;
 				bool keep = false;
 				uint64_t vd = 0;
-				int32_t k = 0;
+				int32_t k = 0, t = 0;
 				if (j < n_x) {
 					vd = X_VD[j], k = X_K[j];
+					if constexpr (TR) t = X_T[j];
 					keep = !in_ranges(ILO, IHI, n_i, vd, i_min, i_max);
 				}
 				const uint32_t m = __ballot_sync(FULL, keep);
@@ -590,6 +704,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 				if (keep) {
 					const int32_t pos = n_kx + __popc(m & lanemask_lt()) + lower_bound_u64(BA_VD, n_b, vd);
 					A_VD[pos] = vd, A_K[pos] = k;
+					if constexpr (TR) A_T[pos] = t;
 				}
 				n_kx += __popc(m);
 			}
@@ -605,6 +720,7 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 					below = (int32_t)(info >> 32) + __popc((uint32_t)info & ((1u << (px & 31)) - 1));
 				}
 				A_VD[j + below] = vd, A_K[j + below] = BA_K[j];
+				if constexpr (TR) A_T[j + below] = BA_T[j];
 			}
 			n_new = n_kx + n_b;
 			__syncwarp();
@@ -626,7 +742,35 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 		if (p.steps_out) p.steps_out[r] = steps;
 		if (p.w_out) p.w_out[r] = W;
 	}
+	if constexpr (TR) {
+		// walk the trace records from the end state back to the start (parents precede their
+		// children, so every step lowers the index), then write the first max_nv vertices
+		if (lane == 0) {
+			int32_t nvp = 0;
+			const bool ok = st == ST_OK && dist >= 0 && tr_t >= 0 && tr_t < n_log;
+			if (ok) {
+				for (int32_t t = tr_t; t >= 0; ++nvp) {
+					const int32_t par = (int32_t)TLOG[t].y;
+					t = par < t ? par : -1;
+				}
+				int32_t pos = nvp - 1;
+				const int64_t row = (int64_t)r * p.max_nv;
+				for (int32_t t = tr_t; t >= 0 && pos >= 0; --pos) {
+					const uint2 e = TLOG[t];
+					if (pos < p.max_nv) {
+						const bool root = e.x == 0xffffffffu;
+						p.path_v[row + pos] = root ? v0 : (int32_t)__ldg(g.arc + e.x).x;
+						p.path_arc[row + pos] = root ? -1 : (int32_t)e.x;
+					}
+					t = (int32_t)e.y < t ? (int32_t)e.y : -1;
+				}
+			}
+			p.path_n[r] = nvp;
+			p.end_off[r] = ok ? tr_k : -1;
+		}
+	}
 }
+
 #undef A_VD
 #undef X_VD
 #undef BA_VD
@@ -645,6 +789,19 @@ __device__ __noinline__ void align_read(const KParams &p, int32_t r, uint8_t *ws
 #undef E_K
 #undef F_K
 #undef N_K
+#undef A_T
+#undef X_T
+#undef BA_T
+#undef E_T
+#undef F_T
+#undef N_T
+#undef BK
+#undef TLOG
+
+__device__ __forceinline__ void align_read(const KParams &p, int32_t r, uint8_t *wsb, int32_t ql_cap, int32_t level)
+{
+	align_read_t<false>(p, r, wsb, ql_cap, level);
+}
 
 // Plain form: one warp per queue position, arena offsets per read (main.cu:151-236 layout).
 __global__ void __launch_bounds__(256, 3) k_align_plain(const __grid_constant__ KParams p)
@@ -653,6 +810,15 @@ __global__ void __launch_bounds__(256, 3) k_align_plain(const __grid_constant__ 
 	if (gw >= p.n_order) return;
 	const int32_t r = p.order[gw];
 	align_read(p, r, p.ws + p.slot_off[gw], p.r.ql[r], p.level);
+}
+
+// Traceback form: the plain form's launch shape, arenas with the trace arrays, paths written out.
+__global__ void __launch_bounds__(256, 2) k_align_trace(const __grid_constant__ KParams p)
+{
+	const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+	if (gw >= p.n_order) return;
+	const int32_t r = p.order[gw];
+	align_read_t<true>(p, r, p.ws + p.slot_off[gw], p.r.ql[r], p.level);
 }
 
 // Persistent form: each warp owns one arena (sized for ql_cap) and pulls reads from the

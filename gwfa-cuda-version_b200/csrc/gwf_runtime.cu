@@ -792,6 +792,122 @@ extern "C" int32_t gwf_ed(void *km, const gwf_graph_t *g, int32_t ql, const char
 	return dist;
 }
 
+// ------------------------------------------------------------------ traceback batches
+struct TraceBufs { // per-device path outputs of gwf_ed_batch_path
+	DBuf end_off, path_n, path_v, path_arc;
+};
+static std::unordered_map<int, TraceBufs *> g_trace_bufs;
+
+// Traceback launches over the reads in ids at one arena class: one warp per read with the plain
+// form's per-read arenas (the trace arrays after the alignment arrays), in chunks that fit the
+// budget.
+static int launch_trace(Engine &E, KParams p, Batch &B, const std::vector<int32_t> &ids, int level, int *launches)
+{
+	const int64_t budget = std::max<int64_t>(E.mem_budget, (int64_t)E.ws.cap);
+	size_t start = 0;
+	std::vector<int64_t> offs;
+	while (start < ids.size()) {
+		offs.clear();
+		int64_t used = 0;
+		size_t end = start;
+		while (end < ids.size()) {
+			const Caps c = caps_for(B.h_ql[(size_t)ids[end]], level, p.dens_milli);
+			const int64_t sz = tr_layout(c, ws_layout(c).total).total;
+			if (used + sz > budget && end > start) break;
+			offs.push_back(used);
+			used += sz;
+			++end;
+		}
+		int rc;
+		if ((rc = E.ws.ensure((size_t)used))) return rc;
+		if ((rc = E.slot_off.ensure(8 * offs.size()))) return rc;
+		if ((rc = E.order.ensure(4 * (end - start)))) return rc;
+		CK(cudaMemcpyAsync(E.slot_off.p, offs.data(), 8 * offs.size(), cudaMemcpyHostToDevice, E.stream));
+		CK(cudaMemcpyAsync(E.order.p, ids.data() + start, 4 * (end - start), cudaMemcpyHostToDevice, E.stream));
+		p.order = (const int32_t *)E.order.p;
+		p.n_order = (int32_t)(end - start);
+		p.ws = (uint8_t *)E.ws.p;
+		p.slot_off = (const int64_t *)E.slot_off.p;
+		p.level = level;
+		const int ctas = (p.n_order + kWarpsPerCta - 1) / kWarpsPerCta;
+		k_align_trace<<<ctas, 32 * kWarpsPerCta, 0, E.stream>>>(p);
+		CK(cudaGetLastError());
+		++*launches;
+		// arenas, offsets and order are reused by the next chunk (the copies above are from
+		// pageable memory, staged before they return)
+		CK(cudaStreamSynchronize(E.stream));
+		start = end;
+	}
+	return 0;
+}
+
+extern "C" int gwf_ed_batch_path(const gwf_graph_t *g, int32_t n, const char *seqs, const int64_t *offs,
+                                 const int32_t *ql, const int32_t *v0, int32_t v1, int32_t flags,
+                                 int32_t max_nv, int32_t *dist, int32_t *status, int32_t *end_off,
+                                 int32_t *path_n, int32_t *path_v, int32_t *path_arc)
+{
+	if (n < 0 || max_nv < 0 ||
+	    (n > 0 && (!seqs || !offs || !ql || !v0 || !dist || !status || !end_off || !path_n ||
+	               (max_nv > 0 && (!path_v || !path_arc))))) {
+		gwf_set_error("bad batch arguments");
+		return GWF_E_BAD_INPUT;
+	}
+	GraphDev *G;
+	Engine *E;
+	int rc = prepare(g, nullptr, &G, &E);
+	if (rc) return rc;
+	if (v1 >= 0 && (uint32_t)v1 >= G->n_vtx) {
+		gwf_set_error("v1 out of range");
+		return GWF_E_BAD_INPUT;
+	}
+	if (n == 0) return 0;
+	std::lock_guard<std::mutex> lk(g_batch_mu);
+	Batch *&B = g_scratch_batches[E->device];
+	if (!B) B = new Batch;
+	TraceBufs *&T = g_trace_bufs[E->device];
+	if (!T) T = new TraceBufs;
+	const size_t cells = (size_t)n * (size_t)std::max(max_nv, 1);
+	if ((rc = gwf_batch_load(*E, *B, n, seqs, offs, ql, v0, v1))) return rc;
+	if ((rc = T->end_off.ensure(4 * (size_t)n)) || (rc = T->path_n.ensure(4 * (size_t)n)) ||
+	    (rc = T->path_v.ensure(4 * cells)) || (rc = T->path_arc.ensure(4 * cells)) ||
+	    (rc = E->retry_list.ensure(4 * (size_t)n + 4)) || (rc = E->retry_n.ensure(16)) ||
+	    (rc = E->h_small.ensure(4 * (size_t)n + 64)))
+		return rc;
+	KParams p = base_params(*E, *G, *B, flags);
+	p.end_off = (int32_t *)T->end_off.p;
+	p.path_n = (int32_t *)T->path_n.p;
+	p.path_v = (int32_t *)T->path_v.p;
+	p.path_arc = (int32_t *)T->path_arc.p;
+	p.max_nv = max_nv;
+	int launches = 0;
+	if ((rc = enqueue_pack(*E, *B))) return rc;
+	std::vector<int32_t> ids((size_t)n);
+	std::iota(ids.begin(), ids.end(), 0);
+	for (int level = 0; level <= kMaxLevel && !ids.empty(); ++level) {
+		CK(cudaMemsetAsync(E->retry_n.p, 0, 4, E->stream));
+		KParams q = p;
+		if (level == kMaxLevel) q.retry_list = nullptr; // last class: keep GWF_E_CAPACITY
+		if ((rc = launch_trace(*E, q, *B, ids, level, &launches))) return rc;
+		CK(cudaMemcpyAsync(E->h_small.p, E->retry_n.p, 4, cudaMemcpyDeviceToHost, E->stream));
+		CK(cudaStreamSynchronize(E->stream));
+		const int32_t nr = level == kMaxLevel ? 0 : *(int32_t *)E->h_small.p;
+		ids.resize((size_t)nr);
+		if (nr == 0) break;
+		CK(cudaMemcpyAsync(E->h_small.p, E->retry_list.p, 4 * (size_t)nr, cudaMemcpyDeviceToHost, E->stream));
+		CK(cudaStreamSynchronize(E->stream));
+		memcpy(ids.data(), E->h_small.p, 4 * (size_t)nr);
+		std::sort(ids.begin(), ids.end());
+	}
+	if ((rc = gwf_batch_fetch(*E, *B, dist, status))) return rc;
+	CK(cudaMemcpy(end_off, T->end_off.p, 4 * (size_t)n, cudaMemcpyDeviceToHost));
+	CK(cudaMemcpy(path_n, T->path_n.p, 4 * (size_t)n, cudaMemcpyDeviceToHost));
+	if (max_nv > 0) {
+		CK(cudaMemcpy(path_v, T->path_v.p, 4 * cells, cudaMemcpyDeviceToHost));
+		CK(cudaMemcpy(path_arc, T->path_arc.p, 4 * cells, cudaMemcpyDeviceToHost));
+	}
+	return 0;
+}
+
 // ------------------------------------------------------------------ resident batches
 struct gwf_batch_s {
 	const gwf_graph_t *g;

@@ -106,6 +106,27 @@ int gwf_ed_batch_concat(const gwf_graph_t *g, int32_t n, const char *seqs, const
                         const int32_t *ql, const int32_t *v0, int32_t v1, uint32_t max_lag,
                         int32_t *dist, int32_t *status, const gwf_batch_opts_t *opt);
 
+/* ---- traceback: the alignment path ----
+ * The reference computes distances only: gwf_ed's traceback argument is unused there
+ * (README.md:117-118; no path output in gwfa.h:95), so this entry point has no counterpart; it
+ * stands where upstream GWFA returns its path. Reads as in gwf_ed_batch_concat, flags as in
+ * gwf_batch_opts_t.flags; the distances equal gwf_ed_batch_concat's. For read i (rows are max_nv
+ * wide, row i starts at i * max_nv):
+ *   path_n[i]           vertices on the path; only the first min(path_n[i], max_nv) are written
+ *   path_v[row + j]     j-th vertex, path_v[row] = v0[i]
+ *   path_arc[row + j]   index in g->arc (as sorted by gwf_ed_index) of the arc from vertex j-1
+ *                       to vertex j; the alignment enters vertex j at that arc's overlap
+ *                       offset o; -1 for j = 0
+ *   end_off[i]          offset in the last vertex of the last base the alignment consumes
+ * The path spells seq[v0][0 ..] then seq[w][o ..] for each later vertex, through end_off of the
+ * last; aligning the read end to end against that text costs at most dist[i] (exactly dist[i]
+ * with GWF_F_EXACT_START and v1 = -1). path_n[i] = 0 and end_off[i] = -1 when the read has no
+ * alignment or a non-OK status. Synchronous; returns 0 or a negative GWF_E_* code. */
+int gwf_ed_batch_path(const gwf_graph_t *g, int32_t n, const char *seqs, const int64_t *offs,
+                      const int32_t *ql, const int32_t *v0, int32_t v1, int32_t flags, int32_t max_nv,
+                      int32_t *dist, int32_t *status, int32_t *end_off, int32_t *path_n,
+                      int32_t *path_v, int32_t *path_arc);
+
 /* ---- device-resident batches (inputs uploaded once; used to time the kernel alone) ---- */
 typedef struct gwf_batch_s gwf_batch_t;
 gwf_batch_t *gwf_batch_create(const gwf_graph_t *g, int32_t n, const char *seqs,
