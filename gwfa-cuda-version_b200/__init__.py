@@ -29,6 +29,7 @@ GWF_E_NOMEM = -9
 GWF_E_BUSY = -10
 
 GWF_F_EXACT_START = 1
+GWF_F_MAX_LAG = 2
 MODE_AUTO, MODE_PLAIN, MODE_PERSISTENT = 0, 1, 2
 
 

@@ -2,18 +2,21 @@
 // (main.cu:360-750): the same options and arguments, one edit distance per read on stdout, in
 // input order. The alignment runs through the library's batch entry point on the device.
 //
-//   gwf-b200 [-p] [-s STR] [-l INT] [-m persistent|plain] [-x] <target.gfa> <query.fa|fq[.gz]>
+//   gwf-b200 [-p] [-s STR] [-l INT] [-m persistent|plain] [-x] [-t] <target.gfa> <query.fa|fq[.gz]>
 //
 //   -p   print the graph (gwf_graph_print format) and exit     (main.cu:382-387, 354-359)
 //   -s   starting segment name [first]; a trailing + or - picks the strand (main.cu:399-407)
 //   -l   max lag; accepted and ignored, as in the reference     (main.cu:371, 377)
 //   -m   execution form [persistent]
 //   -x   exact start state (GWF_F_EXACT_START)
+//   -t   traceback: after each distance, the end offset and the vertex path (no reference
+//        counterpart; the reference's traceback argument is unused, README.md:117-118)
 //
 // Every read is aligned from offset 0 of the start segment (vertex 0 of the converted graph),
 // as the reference kernel does (main.cu:217). Timing and counts go to stderr.
 #include <zlib.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -76,13 +79,14 @@ void usage()
 	fprintf(stderr, "  -p        output GFA in the forward strand\n");
 	fprintf(stderr, "  -m STR    execution form: persistent or plain [persistent]\n");
 	fprintf(stderr, "  -x        exact start state (no reference start-state rule)\n");
+	fprintf(stderr, "  -t        traceback: print distance, end offset and vertex path per read\n");
 }
 
 } // namespace
 
 int main(int argc, char *argv[])
 {
-	bool print_graph = false, exact = false;
+	bool print_graph = false, exact = false, trace = false;
 	const char *sname = nullptr;
 	int32_t mode = GWF_MODE_PERSISTENT;
 	uint32_t max_lag = 0;
@@ -91,6 +95,7 @@ int main(int argc, char *argv[])
 		const char *a = argv[i];
 		if (!strcmp(a, "-p")) print_graph = true;
 		else if (!strcmp(a, "-x")) exact = true;
+		else if (!strcmp(a, "-t")) trace = true;
 		else if (!strcmp(a, "-s") && i + 1 < argc) sname = argv[++i];
 		else if (!strcmp(a, "-l") && i + 1 < argc) max_lag = (uint32_t)atoi(argv[++i]);
 		else if (!strcmp(a, "-m") && i + 1 < argc) {
@@ -141,9 +146,38 @@ int main(int argc, char *argv[])
 	opt.mode = mode;
 	opt.flags = exact ? GWF_F_EXACT_START : 0;
 	const auto t0 = std::chrono::steady_clock::now();
-	const int rc = n > 0 ? gwf_ed_batch_concat(g, n, cat.data(), offs.data(), lens.data(), v0.data(), -1, max_lag,
-	                                           dist.data(), status.data(), &opt)
-	                     : 0;
+	std::vector<std::string> paths;
+	int rc = 0;
+	if (trace) {
+		// chunks of reads; a row of max_nv vertices, widened for a chunk whose paths are longer
+		paths.resize((size_t)n);
+		const int32_t chunk = 8192;
+		for (int32_t c0 = 0; c0 < n && !rc; c0 += chunk) {
+			const int32_t m = std::min(chunk, n - c0);
+			int32_t max_nv = 256;
+			std::vector<int32_t> eo((size_t)m), pn((size_t)m), pv, pa;
+			for (int pass = 0; pass < 2 && !rc; ++pass) {
+				pv.assign((size_t)m * (size_t)max_nv, 0), pa.assign((size_t)m * (size_t)max_nv, 0);
+				rc = gwf_ed_batch_path(g, m, cat.data(), offs.data() + c0, lens.data() + c0, v0.data() + c0, -1,
+				                       opt.flags, max_nv, dist.data() + c0, status.data() + c0, eo.data(), pn.data(),
+				                       pv.data(), pa.data());
+				const int32_t need = m ? *std::max_element(pn.begin(), pn.end()) : 0;
+				if (need <= max_nv) break;
+				max_nv = need;
+			}
+			for (int32_t j = 0; j < m && !rc; ++j) {
+				std::string &o = paths[(size_t)(c0 + j)];
+				o = "\t" + std::to_string(eo[(size_t)j]) + "\t";
+				for (int32_t k = 0; k < pn[(size_t)j] && k < max_nv; ++k) {
+					if (k) o += ',';
+					o += std::to_string(pv[(size_t)j * max_nv + k]);
+				}
+			}
+		}
+	} else if (n > 0) {
+		rc = gwf_ed_batch_concat(g, n, cat.data(), offs.data(), lens.data(), v0.data(), -1, max_lag, dist.data(),
+		                         status.data(), &opt);
+	}
 	const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 	if (rc) {
 		fprintf(stderr, "ERROR: batch alignment failed (%d): %s\n", rc, gwf_last_error());
@@ -152,7 +186,8 @@ int main(int argc, char *argv[])
 	}
 	int32_t bad = 0;
 	for (int32_t j = 0; j < n; ++j) {
-		printf("%d\n", dist[(size_t)j]);
+		if (trace) printf("%d%s\n", dist[(size_t)j], paths[(size_t)j].c_str());
+		else printf("%d\n", dist[(size_t)j]);
 		if (status[(size_t)j] != GWF_OK) ++bad;
 	}
 	fprintf(stderr, "[gwf-b200] aligned in %.6f s (%d reads with a per-read error status)\n", el, bad);

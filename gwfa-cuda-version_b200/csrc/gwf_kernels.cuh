@@ -18,6 +18,8 @@ struct KParams {
 	int32_t dens_milli;     // graph density for arena sizing
 	int32_t ql_cap;         // persistent: arenas sized for this read length
 	int32_t flags;          // bit 0: exact start (no reference start-state quirk)
+	int32_t max_lag;        // > 0: after each step drop the states whose query position lags the
+	                        // furthest state's by more than max_lag (0 = keep all)
 	int32_t *dist;
 	int32_t *status;
 	int32_t *retry_list;    // reads that overflowed their arena
@@ -93,8 +95,10 @@ constexpr int32_t kRadixMin = 128;
 // The arena capacities are those of caps_for(min(ql, ql_cap), level): the arena at wsb must hold
 // them (callers size it for ql_cap, or for the read itself). With TR, the arena also holds
 // tr_layout's arrays after ws_layout's, every state carries the id of the trace record of the
-// last arc it crossed, and the read's path is written to p.path_*.
-template <bool TR>
+// last arc it crossed, and the read's path is written to p.path_*. With LAG, each step ends with
+// the lag pruning of p.max_lag (a separate instantiation, so that the distance kernel's code is
+// untouched by it).
+template <bool TR, bool LAG>
 __device__ __noinline__ void align_read_t(const KParams &p, int32_t r, uint8_t *wsb, int32_t ql_cap, int32_t level)
 {
 	const int lane = threadIdx.x & 31;
@@ -726,6 +730,38 @@ __device__ __noinline__ void align_read_t(const KParams &p, int32_t r, uint8_t *
 			__syncwarp();
 		}
 		n_a = n_new;
+		if (LAG && n_a > 0) {
+			// lag pruning, where the reference's commented-out call sits (gwf-ed.cu:1286-1287):
+			// keep the states whose query position d + k is within max_lag of the furthest
+			int32_t far = INT32_MIN;
+			for (int32_t j = lane; j < n_a; j += 32) {
+				const int32_t i = vd_d(A_VD[j]) + A_K[j];
+				far = i > far ? i : far;
+			}
+			far = __reduce_max_sync(FULL, far);
+			const int32_t lo = far - p.max_lag;
+			int32_t n_keep = 0;
+			for (int32_t base = 0; base < n_a; base += 32) {
+				const int32_t j = base + lane;
+				uint64_t vd = 0;
+				int32_t k = 0, t = 0;
+				bool keep = false;
+				if (j < n_a) {
+					vd = A_VD[j], k = A_K[j];
+					if constexpr (TR) t = A_T[j];
+					keep = vd_d(vd) + k >= lo;
+				}
+				const uint32_t m = __ballot_sync(FULL, keep);
+				if (keep) {
+					const int32_t pos = n_keep + __popc(m & lanemask_lt());
+					A_VD[pos] = vd, A_K[pos] = k;
+					if constexpr (TR) A_T[pos] = t;
+				}
+				n_keep += __popc(m);
+			}
+			n_a = n_keep;
+			__syncwarp();
+		}
 		if (n_a == 0) break; // wavefront emptied: no alignment (gwf-ed.cu:1313, 1336)
 		if (n_a > c.a) {
 			st = ST_CAPACITY;
@@ -800,7 +836,8 @@ __device__ __noinline__ void align_read_t(const KParams &p, int32_t r, uint8_t *
 
 __device__ __forceinline__ void align_read(const KParams &p, int32_t r, uint8_t *wsb, int32_t ql_cap, int32_t level)
 {
-	align_read_t<false>(p, r, wsb, ql_cap, level);
+	if (p.max_lag > 0) align_read_t<false, true>(p, r, wsb, ql_cap, level);
+	else align_read_t<false, false>(p, r, wsb, ql_cap, level);
 }
 
 // Plain form: one warp per queue position, arena offsets per read (main.cu:151-236 layout).
@@ -818,7 +855,7 @@ __global__ void __launch_bounds__(256, 2) k_align_trace(const __grid_constant__ 
 	const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
 	if (gw >= p.n_order) return;
 	const int32_t r = p.order[gw];
-	align_read_t<true>(p, r, p.ws + p.slot_off[gw], p.r.ql[r], p.level);
+	align_read_t<true, false>(p, r, p.ws + p.slot_off[gw], p.r.ql[r], p.level);
 }
 
 // Persistent form: each warp owns one arena (sized for ql_cap) and pulls reads from the
@@ -962,6 +999,7 @@ __global__ void __launch_bounds__(256, 3) k_serve(const __grid_constant__ SrvPar
 			lp.r.n = 1;
 			lp.dens_milli = p.dens_milli;
 			lp.flags = p.flags;
+			lp.max_lag = 0;
 			lp.dist = &hdr->dist;
 			lp.status = &hdr->status;
 			align_read(lp, 0, ab + qb, ql, level);

@@ -555,7 +555,8 @@ static int launch_level0_graph(Engine &E, Batch &B, const KParams &p, int ctas_p
 	int rc;
 	if ((rc = plan_persistent(E, B.n, B.max_ql, 0, ctas_per_sm, p.dens_milli, &pl))) return rc;
 	const uint64_t key[8] = {B.generation, (uint64_t)(uintptr_t)E.ws.p, (uint64_t)pl.slot, (uint64_t)pl.ctas,
-	                         (uint64_t)(uint32_t)p.flags, (uint64_t)(uintptr_t)E.retry_n.p,
+	                         (uint64_t)(uint32_t)p.flags | (uint64_t)(uint32_t)p.max_lag << 32,
+	                         (uint64_t)(uintptr_t)E.retry_n.p,
 	                         (uint64_t)(uintptr_t)E.h_small.p, (uint64_t)(uintptr_t)E.retry_list.p};
 	if (!B.gexec || memcmp(key, B.gkey, sizeof key) != 0) {
 		if (B.gexec) cudaGraphExecDestroy(B.gexec), B.gexec = nullptr;
@@ -588,7 +589,7 @@ static int launch_level0_graph(Engine &E, Batch &B, const KParams &p, int ctas_p
 }
 
 int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t flags,
-                   int ctas_per_sm, float *ms, int *launches_out, int use_graph)
+                   int ctas_per_sm, float *ms, int *launches_out, int use_graph, int32_t max_lag)
 {
 	int launches = 0, rc;
 	if (B.n == 0) {
@@ -600,6 +601,7 @@ int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t
 	    (rc = E.h_small.ensure(4 * (size_t)B.n + 64)))
 		return rc;
 	KParams p = base_params(E, G, B, flags);
+	p.max_lag = max_lag > 0 ? max_lag : 0;
 	if (mode == GWF_MODE_AUTO && ctas_per_sm <= 0) { // autotuned shape for the dominant length bucket
 		int32_t f = 0, c = 0;
 		if (gwf_tune_lookup(E.device, B.dom_bucket, &f, &c)) mode = f, ctas_per_sm = c;
@@ -716,7 +718,7 @@ extern "C" int gwf_ed_batch_concat(const gwf_graph_t *g, int32_t n, const char *
                                    int32_t v1, uint32_t max_lag, int32_t *dist, int32_t *status,
                                    const gwf_batch_opts_t *opt)
 {
-	(void)max_lag; // accepted and ignored, as in the reference (gwf-ed.cu:1286-1287)
+	// max_lag is ignored, as in the reference (gwf-ed.cu:1286-1287), unless GWF_F_MAX_LAG is set
 	if (n < 0 || (n > 0 && (!seqs || !offs || !ql || !v0 || !dist))) {
 		gwf_set_error("bad batch arguments");
 		return GWF_E_BAD_INPUT;
@@ -736,7 +738,8 @@ extern "C" int gwf_ed_batch_concat(const gwf_graph_t *g, int32_t n, const char *
 	const int32_t mode = opt ? opt->mode : GWF_MODE_AUTO;
 	const int32_t flags = opt ? opt->flags : 0;
 	const int32_t cps = opt ? opt->ctas_per_sm : 0;
-	if ((rc = gwf_batch_exec(*E, *G, *B, mode, flags, cps, nullptr, nullptr, opt ? opt->use_graph : 0)))
+	const int32_t lag = (flags & GWF_F_MAX_LAG) ? (int32_t)std::min<uint32_t>(max_lag, INT32_MAX) : 0;
+	if ((rc = gwf_batch_exec(*E, *G, *B, mode, flags, cps, nullptr, nullptr, opt ? opt->use_graph : 0, lag)))
 		return rc;
 	std::vector<int32_t> st;
 	if (!status) st.resize((size_t)n), status = st.data();

@@ -65,7 +65,7 @@ int gwf_select_device(int want, int *dev_out);
 int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64_t *offs,
                    const int32_t *ql, const int32_t *v0, int32_t v1);
 int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t flags,
-                   int ctas_per_sm, float *ms, int *launches_out, int use_graph = 0);
+                   int ctas_per_sm, float *ms, int *launches_out, int use_graph = 0, int32_t max_lag = 0);
 int gwf_batch_fetch(Engine &E, Batch &B, int32_t *dist, int32_t *status);
 namespace gwfb {
 struct KParams;

@@ -38,8 +38,9 @@ typedef struct {
 #define GWF_OK               0
 #define GWF_NO_ALIGNMENT    (-1) /* distance value: wavefront emptied (gwf-ed.cu:1336) */
 #define GWF_E_BAD_INPUT     (-2) /* ql <= 0, v0/v1 out of range, null pointer */
-#define GWF_E_UNSUPPORTED   (-3) /* traceback != 0: the reference has none (max_lag is accepted
-                                   * and ignored, as the reference ignores it) */
+#define GWF_E_UNSUPPORTED   (-3) /* gwf_ed with traceback != 0: the reference has none (paths come
+                                   * from gwf_ed_batch_path); max_lag is accepted and ignored, as the
+                                   * reference ignores it, unless GWF_F_MAX_LAG is set */
 #define GWF_E_CAPACITY      (-4) /* read did not fit the largest wavefront arena class */
 #define GWF_E_CUDA          (-5) /* CUDA runtime failure or no usable B200 device */
 #define GWF_E_NOT_INDEXED   (-6) /* gwf_ed_index was not called for this graph */
@@ -57,6 +58,12 @@ typedef struct {
                                    candidates with k = -1 (uint32_t vl, gwf-ed.cu:895,993), so an
                                    alignment cannot begin with an insertion. Both add cost to
                                    some reads. Default off = reference-identical distances. */
+#define GWF_F_MAX_LAG       0x2 /* apply the batch call's max_lag (no reference counterpart: the
+                                   reference's prune call is commented out, gwf-ed.cu:1286-1287).
+                                   After each score step, the states whose query position d + k
+                                   is more than max_lag behind the furthest state's are dropped.
+                                   A heuristic: distances can only grow, or become -1 when no
+                                   state is left. Off = max_lag ignored, as in the reference. */
 
 /* execution forms */
 #define GWF_MODE_AUTO        0 /* persistent cost-ordered queue */

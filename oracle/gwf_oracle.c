@@ -24,6 +24,7 @@
  * The independent ground truth gwfo_dp() is at the end of the file.
  */
 #define _GNU_SOURCE
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 #include <stdio.h>
@@ -52,7 +53,7 @@ static inline uint64_t gen_vd(uint32_t v, int32_t d) /* gwf-ed.cu:80-83 */
 
 typedef struct {
 	const gwf_graph_t *g;
-	int32_t ql, v1, opts;
+	int32_t ql, v1, opts, max_lag;
 	const char *q;
 	/* reference arena caps (main.cu:498-505) */
 	int64_t max_a, max_B, max_A, max_intv, max_tmp, max_swap, max_ooo;
@@ -339,6 +340,22 @@ static int32_t o_dedup(ows_t *w, int32_t n_a)
 	return n_a;
 }
 
+/* Lag pruning (no reference body: the call at gwf-ed.cu:1286-1287 is commented out and gwfa.h
+ * declares no gwf_prune). The product's rule: keep the states whose query position d + k is
+ * within max_lag of the furthest state's, in order. */
+static int32_t o_prune(ows_t *w, int32_t n_a)
+{
+	int32_t i, far = INT32_MIN, kw = 0;
+	for (i = 0; i < n_a; ++i) {
+		int32_t x = (int32_t)w->a_vd[i] - SHIFT + w->a_k[i];
+		if (x > far) far = x;
+	}
+	for (i = 0; i < n_a; ++i)
+		if ((int32_t)w->a_vd[i] - SHIFT + w->a_k[i] >= far - w->max_lag)
+			w->a_vd[kw] = w->a_vd[i], w->a_k[kw] = w->a_k[i], w->a_xo[kw] = w->a_xo[i], ++kw;
+	return kw;
+}
+
 /* ------------------------------------------------------------------ queues */
 static void A_push(ows_t *w, uint64_t vd, int32_t k, uint32_t xo) /* static_A_pushp :841-857 */
 {
@@ -523,6 +540,7 @@ static int o_extend(ows_t *w, int32_t *end_v, int32_t *end_off)
 		w->a_vd[i] = w->B[i].vd, w->a_k[i] = w->B[i].k, w->a_xo[i] = w->B[i].xo;
 	w->n_a = w->n_B, w->n_B = 0;
 	if (do_dedup) w->n_a = o_dedup(w, w->n_a);
+	if (w->max_lag > 0 && w->n_a > 0) w->n_a = o_prune(w, w->n_a);
 	return 0;
 }
 
@@ -534,14 +552,14 @@ static uint32_t next_pow2_u32(uint32_t x) /* main.cu:279-292 */
 	return x + 1;
 }
 
-/* gwf_ed (gwf-ed.cu:1292-1337) */
-int32_t gwfo_ed(const gwf_graph_t *g, int32_t ql, const char *q, int32_t v0, int32_t v1,
-                int32_t opts, gwfo_stats_t *st)
+/* gwf_ed (gwf-ed.cu:1292-1337); max_lag > 0 adds o_prune after each step */
+int32_t gwfo_ed_lag(const gwf_graph_t *g, int32_t ql, const char *q, int32_t v0, int32_t v1,
+                    int32_t opts, int32_t max_lag, gwfo_stats_t *st)
 {
 	ows_t w;
 	int32_t s = 0, end_v = -1, end_off = -1, ret;
 	memset(&w, 0, sizeof(w));
-	w.g = g, w.ql = ql, w.q = q, w.v1 = v1, w.opts = opts;
+	w.g = g, w.ql = ql, w.q = q, w.v1 = v1, w.opts = opts, w.max_lag = max_lag;
 	/* main.cu:498-505 */
 	w.max_a = (uint32_t)(((4 * (size_t)(ql > 0 ? ql : 0) * 0.1) + 1) * 4);
 	w.max_B = 3 * w.max_a + 1;
@@ -569,6 +587,12 @@ int32_t gwfo_ed(const gwf_graph_t *g, int32_t ql, const char *q, int32_t v0, int
 	free(w.intv0), free(w.intv1), free(w.tmp0), free(w.tmp1), free(w.swap0), free(w.swap1);
 	free(w.ooo), free(w.scr), free(w.hk);
 	return ret;
+}
+
+int32_t gwfo_ed(const gwf_graph_t *g, int32_t ql, const char *q, int32_t v0, int32_t v1,
+                int32_t opts, gwfo_stats_t *st)
+{
+	return gwfo_ed_lag(g, ql, q, v0, v1, opts, 0, st);
 }
 
 /* ------------------------------------------------------------------ index (main.cu:242-270) */

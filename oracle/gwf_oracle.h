@@ -50,6 +50,10 @@ void gwfo_index_free(gwf_graph_t *g);
 int32_t gwfo_ed(const gwf_graph_t *g, int32_t ql, const char *q, int32_t v0, int32_t v1,
                 int32_t opts, gwfo_stats_t *st);
 
+/* gwfo_ed with the product's lag pruning after each step (max_lag > 0; 0 = gwfo_ed). */
+int32_t gwfo_ed_lag(const gwf_graph_t *g, int32_t ql, const char *q, int32_t v0, int32_t v1,
+                    int32_t opts, int32_t max_lag, gwfo_stats_t *st);
+
 /* Many reads over a thread pool (n_threads <= 0: all online cores). st may be NULL.
  * Returns the number of threads used. */
 int32_t gwfo_ed_batch(const gwf_graph_t *g, int32_t n, const char *seqs, const int64_t *offs,

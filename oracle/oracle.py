@@ -54,6 +54,9 @@ def lib():
         L.gwfo_ed.argtypes = [P, ctypes.c_int32, ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32,
                               ctypes.c_int32, P]
         L.gwfo_ed.restype = ctypes.c_int32
+        L.gwfo_ed_lag.argtypes = [P, ctypes.c_int32, ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32,
+                                  ctypes.c_int32, ctypes.c_int32, P]
+        L.gwfo_ed_lag.restype = ctypes.c_int32
         L.gwfo_ed_batch.argtypes = [P, ctypes.c_int32, P, P, P, P, ctypes.c_int32, ctypes.c_int32, P, P,
                                     ctypes.c_int32]
         L.gwfo_ed_batch.restype = ctypes.c_int32
@@ -95,10 +98,12 @@ class OracleGraph:
     def arcs_sorted(self):
         return [(self._g.arc[i].a >> 32, self._g.arc[i].a & 0xffffffff, self._g.arc[i].o) for i in range(self._g.n_arc)]
 
-    def ed(self, q, v0, v1=-1, exact_start=False):
+    def ed(self, q, v0, v1=-1, exact_start=False, max_lag=0):
+        """max_lag > 0: the product's lag pruning (GWF_F_MAX_LAG) after each step."""
         b = q.encode() if isinstance(q, str) else bytes(q)
         st = Stats()
-        d = lib().gwfo_ed(self.ptr, len(b), b, v0, v1, O_EXACT_START if exact_start else 0, ctypes.byref(st))
+        d = lib().gwfo_ed_lag(self.ptr, len(b), b, v0, v1, O_EXACT_START if exact_start else 0, max_lag,
+                              ctypes.byref(st))
         return d, st
 
     def ed_batch(self, cat, offs, lens, v0, v1=-1, exact_start=False, threads=0, stats=True):

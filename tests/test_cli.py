@@ -58,3 +58,23 @@ def test_scores_equal_reference_gwf_test(form, tmp_path):
             f.write("@%s\n%s\n+\n%s\n" % (n, s, "I" * len(s)))
     out2 = run(gfa, str(fq)).stdout.split()
     assert out2 == out
+
+
+@pytest.mark.gpu
+def test_traceback_option(G):
+    """-t: the distance column equals the plain output; each path starts at vertex 0, follows arcs
+    of the converted graph, and ends at a valid offset of its last vertex."""
+    gfa = os.path.join(GOLD, "graph_1000.gfa")
+    reads = os.path.join(GOLD, "reads_200.fa")
+    plain = run(gfa, reads).stdout.split()
+    lines = run("-t", gfa, reads).stdout.splitlines()
+    assert [ln.split("\t")[0] for ln in lines] == plain
+    g = G.Graph.from_gfa(gfa)
+    g.index()
+    arcs = {(v, w) for v, w, _ in g.arcs()}
+    lens = g.lens()
+    for ln in lines:
+        d, eo, path = ln.split("\t")
+        verts = [int(x) for x in path.split(",")]
+        assert verts[0] == 0 and all((a, b) in arcs for a, b in zip(verts, verts[1:]))
+        assert 0 <= int(eo) < lens[verts[-1]]

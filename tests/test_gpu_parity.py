@@ -164,3 +164,36 @@ def test_graph_captured_runs_equal_stream_runs(G):
     d2, s2 = g.ed_batch((cat, offs, lens), v0, use_graph=1)
     assert np.array_equal(d0, d2) and np.array_equal(s0, s2)
     b.close()
+
+
+@pytest.mark.parametrize("lag", [2, 5, 20])
+def test_lag_pruning_matches_oracle(G, O, lag):
+    """GWF_F_MAX_LAG: the kernels' pruned distances equal the oracle's with the same rule, in both
+    forms and through the captured CUDA graph; without the flag max_lag stays ignored."""
+    w = G.load_workload("config2", n=1000)
+    g = _indexed(G, w["graph"])
+    og = O.OracleGraph.from_graph(w["graph"])
+    reads = (w["cat"], w["offs"], w["lens"])
+    od = [og.ed(bytes(w["cat"][o:o + l]), int(v), max_lag=lag)[0] for o, l, v in zip(w["offs"], w["lens"], w["v0"])]
+    for mode, use_graph in ((G.MODE_PLAIN, 0), (G.MODE_PERSISTENT, 0), (G.MODE_PERSISTENT, 1)):
+        d, st = g.ed_batch(reads, w["v0"], mode=mode, flags=G.GWF_F_MAX_LAG, max_lag=lag, use_graph=use_graph)
+        assert (st == 0).all() and list(d) == od
+    full, _ = g.ed_batch(reads, w["v0"], max_lag=lag)  # flag off: ignored, as in the reference
+    d0, _ = g.ed_batch(reads, w["v0"])
+    assert np.array_equal(full, d0)
+
+
+def test_lag_pruning_random_graphs(G, O):
+    checked = 0
+    for t, (seqs, arcs, v0, v1, q) in enumerate(cases(919, 200, v1_prob=0.3)):
+        lag = 1 + t % 4
+        og = O.OracleGraph(seqs, arcs)
+        od, ost = og.ed(q, v0, v1, max_lag=lag)
+        if ost.flags & O.F_NONTERM:
+            continue
+        g = _indexed(G, G.Graph.from_arrays(seqs, arcs))
+        d, st = g.ed_batch([q], [v0], v1=v1, flags=G.GWF_F_MAX_LAG, max_lag=lag)
+        assert st[0] == 0 and d[0] == od, (seqs, arcs, v0, v1, q, lag, d[0], od)
+        checked += 1
+        g.close()
+    assert checked > 150

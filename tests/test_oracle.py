@@ -88,3 +88,30 @@ def test_oracle_matches_reference_on_synthetic(G, O, name):
     sel = np.array(idx)
     d, st, _ = og.ed_batch(w["cat"], w["offs"][sel], w["lens"][sel], w["v0"][sel])
     assert list(d) == ref
+
+
+def test_lag_pruning_bounds(G, O):
+    """The lag pruning that GWF_F_MAX_LAG enables: a lag beyond the read length changes nothing,
+    and a smaller lag can only raise the distance (or leave no alignment, -1)."""
+    w = G.load_workload("config2", n=300)
+    og = O.OracleGraph.from_graph(w["graph"])
+    grew = 0
+    for i in range(0, 300, 3):
+        q = bytes(w["cat"][w["offs"][i]:w["offs"][i] + w["lens"][i]])
+        v0 = int(w["v0"][i])
+        full, _ = og.ed(q, v0)
+        assert og.ed(q, v0, max_lag=len(q) + 1)[0] == full
+        for lag in (2, 5, 20, 100):
+            d, _ = og.ed(q, v0, max_lag=lag)
+            assert d == -1 or d >= full
+            grew += d != full
+    assert grew > 0  # small lags do prune something on 5-10% error reads
+    for seqs, arcs, v0, v1, q in cases(515, 150, v1_prob=0.3):
+        og2 = O.OracleGraph(seqs, arcs)
+        full, st = og2.ed(q, v0, v1)
+        if st.flags & O.F_NONTERM:
+            continue
+        for lag in (1, 3):
+            d, st2 = og2.ed(q, v0, v1, max_lag=lag)
+            if not st2.flags & O.F_NONTERM:
+                assert d == -1 or full == -1 or d >= full
