@@ -2,11 +2,12 @@
 // (main.cu:360-750): the same options and arguments, one edit distance per read on stdout, in
 // input order. The alignment runs through the library's batch entry point on the device.
 //
-//   gwf-b200 [-p] [-s STR] [-l INT] [-m persistent|plain] [-x] [-t] <target.gfa> <query.fa|fq[.gz]>
+//   gwf-b200 [-p] [-s STR] [-l INT [-P]] [-m persistent|plain] [-x] [-t] <target.gfa> <query.fa|fq[.gz]>
 //
 //   -p   print the graph (gwf_graph_print format) and exit     (main.cu:382-387, 354-359)
 //   -s   starting segment name [first]; a trailing + or - picks the strand (main.cu:399-407)
 //   -l   max lag; accepted and ignored, as in the reference     (main.cu:371, 377)
+//   -P   apply -l: lag pruning (GWF_F_MAX_LAG; no reference counterpart); -t does not prune
 //   -m   execution form [persistent]
 //   -x   exact start state (GWF_F_EXACT_START)
 //   -t   traceback: after each distance, the end offset and the vertex path (no reference
@@ -74,7 +75,8 @@ void usage()
 {
 	fprintf(stderr, "Usage: gwf-b200 [options] <target.gfa> <query.fa>\n");
 	fprintf(stderr, "Options:\n");
-	fprintf(stderr, "  -l INT    max lag behind the furthest wavefront; accepted and ignored [0]\n");
+	fprintf(stderr, "  -l INT    max lag behind the furthest wavefront; ignored unless -P [0]\n");
+	fprintf(stderr, "  -P        apply -l: prune states more than -l bases behind the furthest (not with -t)\n");
 	fprintf(stderr, "  -s STR    starting segment name, + or - appended for the strand [first, +]\n");
 	fprintf(stderr, "  -p        output GFA in the forward strand\n");
 	fprintf(stderr, "  -m STR    execution form: persistent or plain [persistent]\n");
@@ -86,7 +88,7 @@ void usage()
 
 int main(int argc, char *argv[])
 {
-	bool print_graph = false, exact = false, trace = false;
+	bool print_graph = false, exact = false, trace = false, prune = false;
 	const char *sname = nullptr;
 	int32_t mode = GWF_MODE_PERSISTENT;
 	uint32_t max_lag = 0;
@@ -96,6 +98,7 @@ int main(int argc, char *argv[])
 		if (!strcmp(a, "-p")) print_graph = true;
 		else if (!strcmp(a, "-x")) exact = true;
 		else if (!strcmp(a, "-t")) trace = true;
+		else if (!strcmp(a, "-P")) prune = true;
 		else if (!strcmp(a, "-s") && i + 1 < argc) sname = argv[++i];
 		else if (!strcmp(a, "-l") && i + 1 < argc) max_lag = (uint32_t)atoi(argv[++i]);
 		else if (!strcmp(a, "-m") && i + 1 < argc) {
@@ -144,7 +147,7 @@ int main(int argc, char *argv[])
 	gwf_batch_opts_t opt;
 	memset(&opt, 0, sizeof opt);
 	opt.mode = mode;
-	opt.flags = exact ? GWF_F_EXACT_START : 0;
+	opt.flags = (exact ? GWF_F_EXACT_START : 0) | (prune ? GWF_F_MAX_LAG : 0);
 	const auto t0 = std::chrono::steady_clock::now();
 	std::vector<std::string> paths;
 	int rc = 0;

@@ -78,3 +78,14 @@ def test_traceback_option(G):
         verts = [int(x) for x in path.split(",")]
         assert verts[0] == 0 and all((a, b) in arcs for a, b in zip(verts, verts[1:]))
         assert 0 <= int(eo) < lens[verts[-1]]
+
+
+@pytest.mark.gpu
+def test_lag_option(G):
+    """-l alone is ignored, as in the reference; -l with -P prunes (distances never below)."""
+    gfa = os.path.join(GOLD, "graph_1000.gfa")
+    reads = os.path.join(GOLD, "reads_200.fa")
+    base = np.array(run(gfa, reads).stdout.split(), dtype=np.int64)
+    assert np.array_equal(np.array(run("-l", "3", gfa, reads).stdout.split(), dtype=np.int64), base)
+    pruned = np.array(run("-l", "3", "-P", gfa, reads).stdout.split(), dtype=np.int64)
+    assert ((pruned >= base) | (pruned == -1)).all()
