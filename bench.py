@@ -327,6 +327,8 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="persistent grid; 0 = occupancy limit")
     ap.add_argument("--graph", type=int, default=1, help="1 = persistent runs replay a captured CUDA graph")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--reads", type=int, default=0,
+                    help="the first N reads of the workload (small profiling cases); 0 = all")
     ap.add_argument("--serving", action="store_true", help="serving benchmark (config5) instead")
     ap.add_argument("--serve-reads", type=int, default=6000)
     ap.add_argument("--serve-budget-gib", type=float, default=64.0)
@@ -358,7 +360,7 @@ def main():
     torch.cuda.set_device(local)
     G = pkg()
     mode = G.MODE_PERSISTENT if args.mode == "persistent" else G.MODE_PLAIN
-    w = G.load_workload(args.workload, seed=shard_seed(args.workload, rank), pinned=True)
+    w = G.load_workload(args.workload, n=args.reads or None, seed=shard_seed(args.workload, rank), pinned=True)
     g = w["graph"]
     g.index()
     n = len(w["lens"])
