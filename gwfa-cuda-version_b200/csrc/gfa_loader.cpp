@@ -22,6 +22,7 @@
 #include <set>
 #include <string>
 #include <string_view>
+#include <thread>
 #include <vector>
 
 #include "../../include/gwfa.h"
@@ -94,6 +95,34 @@ struct NameTable {
 		while (slot[i]) i = (i + 1) & mask;
 		slot[i] = tag(h) | off;
 	}
+	// sizes an empty table for n names (no growth below that)
+	void reserve(size_t n_names, size_t name_bytes)
+	{
+		if (n) return;
+		size_t cap = 1024;
+		while (cap < 2 * (n_names + 1)) cap <<= 1;
+		slot.assign(cap, 0);
+		pool.reserve(pool.size() + name_bytes + 8 * n_names);
+	}
+	void prefetch(uint64_t h) const
+	{
+		if (!slot.empty()) __builtin_prefetch(slot.data() + (h & (slot.size() - 1)));
+	}
+	// second stage: the pool entry of the first slot whose tag agrees (its slot was prefetched)
+	void prefetch_entry(uint64_t h) const
+	{
+		if (slot.empty()) return;
+		const size_t mask = slot.size() - 1;
+		const uint64_t t = tag(h);
+		for (size_t i = (size_t)h & mask, probes = 0; probes < 4; i = (i + 1) & mask, ++probes) {
+			const uint64_t e = slot[i];
+			if (!e) return;
+			if ((e & ~kOffMask) == t) {
+				__builtin_prefetch(pool.data() + (e & kOffMask));
+				return;
+			}
+		}
+	}
 	// appends the name with the given id; the caller has checked that it is absent
 	void add(std::string_view k, uint64_t h, uint32_t id)
 	{
@@ -122,9 +151,9 @@ struct Gfa {
 	std::vector<uint64_t> idx; // per vertex: first << 32 | n
 
 	int64_t find_seg(std::string_view name) const { return names.find(name, NameTable::hash(name)); }
-	uint32_t add_seg(std::string_view name)
+	uint32_t add_seg(std::string_view name) { return add_seg(name, NameTable::hash(name)); }
+	uint32_t add_seg(std::string_view name, uint64_t h)
 	{
-		const uint64_t h = NameTable::hash(name);
 		const int64_t f = names.find(name, h);
 		if (f >= 0) return (uint32_t)f;
 		const uint32_t id = (uint32_t)seg.size();
@@ -216,11 +245,27 @@ void split_tabs(std::string_view line, Fields &out)
 		}
 }
 
-// gfa-io.c:115-220
-int parse_S(Gfa &g, std::string_view line, Fields &f)
+// One S or L line, parsed without touching the graph (the views point into the line), so that
+// lines can be parsed on several threads and applied in file order.
+struct SRec {
+	std::string_view name, seq;
+	uint64_t h;
+	int32_t len;
+	bool has_seq;
+};
+struct LRec {
+	std::string_view v, w;
+	uint64_t hv, hw;
+	int32_t ov, ow, l1, l2;
+	uint8_t oriv, oriw;
+	bool has_l1, has_l2;
+};
+
+// gfa-io.c:115-220; false for a line the reference skips
+bool scan_S(std::string_view line, Fields &f, SRec &r)
 {
 	split_tabs(line, f); // f[0] == "S"
-	if (f.size() < 3) return -1;
+	if (f.size() < 3) return false;
 	const std::string_view name = f[1], sq = f[2];
 	int32_t LN = -1;
 	if (const char *p = find_tag(f, 3, "LN", 'i')) LN = (int32_t)strtol(p, nullptr, 10);
@@ -230,23 +275,28 @@ int parse_S(Gfa &g, std::string_view line, Fields &f)
 		if (LN >= 0) len = LN;
 	} else
 		len = (int32_t)sq.size();
-	uint32_t sid = g.add_seg(name);
-	Seg &s = g.seg[sid];
-	s.len = len;
-	s.has_seq = has_seq;
-	if (has_seq) g.set_seq(s, sq);
-	else s.seq_len = 0;
-	return 0;
+	r.name = name, r.seq = sq, r.h = NameTable::hash(name), r.len = len, r.has_seq = has_seq;
+	return true;
 }
 
-// gfa-io.c:222-324
-int parse_L(Gfa &g, std::string_view line, Fields &f)
+void apply_S(Gfa &g, const SRec &r)
+{
+	const uint32_t sid = g.add_seg(r.name, r.h);
+	Seg &s = g.seg[sid];
+	s.len = r.len;
+	s.has_seq = r.has_seq;
+	if (r.has_seq) g.set_seq(s, r.seq);
+	else s.seq_len = 0;
+}
+
+// gfa-io.c:222-324; false for a line the reference skips
+bool scan_L(std::string_view line, Fields &f, LRec &r)
 {
 	split_tabs(line, f);
-	if (f.size() < 5) return -1;
+	if (f.size() < 5) return false;
 	const std::string_view segv = f[1], segw = f[3];
-	if (f[2].empty() || (f[2][0] != '+' && f[2][0] != '-')) return -2;
-	if (f[4].empty() || (f[4][0] != '+' && f[4][0] != '-')) return -2;
+	if (f[2].empty() || (f[2][0] != '+' && f[2][0] != '-')) return false;
+	if (f[4].empty() || (f[4][0] != '+' && f[4][0] != '-')) return false;
 	int oriv = f[2][0] != '+', oriw = f[4][0] != '+';
 	int32_t ov = 0, ow = 0;
 	size_t tags_from = f.size();
@@ -262,9 +312,9 @@ int parse_L(Gfa &g, std::string_view line, Fields &f)
 			ow = q + 1 < qe && isdigit((unsigned char)q[1]) ? (int32_t)strtol(q + 1, nullptr, 10) : INT32_MAX;
 			ok = true;
 		} else if (q < qe && isdigit((unsigned char)*q)) {
-			char *r;
-			long first = strtol(q, &r, 10);
-			if (r < qe && isupper((unsigned char)*r)) { // CIGAR
+			char *rr;
+			long first = strtol(q, &rr, 10);
+			if (rr < qe && isupper((unsigned char)*rr)) { // CIGAR
 				ov = ow = 0;
 				const char *p = q;
 				do {
@@ -276,30 +326,52 @@ int parse_L(Gfa &g, std::string_view line, Fields &f)
 					++p;
 				} while (p < qe && isdigit((unsigned char)*p));
 				ok = true;
-			} else if (r < qe && *r == ':') {
+			} else if (rr < qe && *rr == ':') {
 				ov = (int32_t)first;
-				ow = r + 1 < qe && isdigit((unsigned char)r[1]) ? (int32_t)strtol(r + 1, nullptr, 10) : INT32_MAX;
+				ow = rr + 1 < qe && isdigit((unsigned char)rr[1]) ? (int32_t)strtol(rr + 1, nullptr, 10) : INT32_MAX;
 				ok = true;
 			}
 		}
 		if (!ok) ov = ow = 0; // unparsable overlap: treated like a missing field (gfa-io.c:277)
 		tags_from = 6;
 	}
-	uint32_t v = g.add_seg(segv) << 1 | (uint32_t)oriv;
-	uint32_t w = g.add_seg(segw) << 1 | (uint32_t)oriw;
-	g.add_arc(v, w, ov, ow, -1, false);
-	if (const char *p = find_tag(f, tags_from, "L1", 'i'))
-		if (ov != INT32_MAX) {
-			int32_t l1 = (int32_t)strtol(p, nullptr, 10);
-			Seg &s = g.seg[v >> 1];
-			if (ov + l1 > s.len) s.len = ov + l1;
-		}
-	if (const char *p = find_tag(f, tags_from, "L2", 'i'))
-		if (ow != INT32_MAX) {
-			int32_t l2 = (int32_t)strtol(p, nullptr, 10);
-			Seg &s = g.seg[w >> 1];
-			if (ow + l2 > s.len) s.len = ow + l2;
-		}
+	r.v = segv, r.w = segw, r.hv = NameTable::hash(segv), r.hw = NameTable::hash(segw);
+	r.ov = ov, r.ow = ow, r.oriv = (uint8_t)oriv, r.oriw = (uint8_t)oriw;
+	const char *p1 = find_tag(f, tags_from, "L1", 'i'), *p2 = find_tag(f, tags_from, "L2", 'i');
+	r.has_l1 = p1 != nullptr, r.has_l2 = p2 != nullptr;
+	r.l1 = p1 ? (int32_t)strtol(p1, nullptr, 10) : 0;
+	r.l2 = p2 ? (int32_t)strtol(p2, nullptr, 10) : 0;
+	return true;
+}
+
+void apply_L(Gfa &g, const LRec &r)
+{
+	const uint32_t v = g.add_seg(r.v, r.hv) << 1 | r.oriv;
+	const uint32_t w = g.add_seg(r.w, r.hw) << 1 | r.oriw;
+	g.add_arc(v, w, r.ov, r.ow, -1, false);
+	if (r.has_l1 && r.ov != INT32_MAX) {
+		Seg &s = g.seg[v >> 1];
+		if (r.ov + r.l1 > s.len) s.len = r.ov + r.l1;
+	}
+	if (r.has_l2 && r.ow != INT32_MAX) {
+		Seg &s = g.seg[w >> 1];
+		if (r.ow + r.l2 > s.len) s.len = r.ow + r.l2;
+	}
+}
+
+int parse_S(Gfa &g, std::string_view line, Fields &f)
+{
+	SRec r;
+	if (!scan_S(line, f, r)) return -1;
+	apply_S(g, r);
+	return 0;
+}
+
+int parse_L(Gfa &g, std::string_view line, Fields &f)
+{
+	LRec r;
+	if (!scan_L(line, f, r)) return -1;
+	apply_L(g, r);
 	return 0;
 }
 
@@ -347,6 +419,8 @@ void fix_symm_add(Gfa &g) // gfa-base.c:303-338
 	for (uint32_t v = 0; v < nvt; ++v) {
 		uint32_t nv = g.arc_n(v), ofs = g.arc_off(v);
 		for (uint32_t i = 0; i < nv; ++i) {
+			// the index entries of the complement lists a few arcs ahead (random accesses)
+			if (ofs + i + 8 < n0) __builtin_prefetch(g.idx.data() + (g.arc[ofs + i + 8].w ^ 1));
 			Arc avi = g.arc[ofs + i];
 			if (avi.del || avi.comp) continue;
 			uint32_t nw = g.arc_n(avi.w ^ 1), ow_ = g.arc_off(avi.w ^ 1), j;
@@ -383,10 +457,15 @@ void fix_arc_len(Gfa &g) // gfa-base.c:249-267
 
 void cleanup(Gfa &g) // gfa-base.c:340-371
 {
+	// deleted segments as a bitmap (small enough to stay in cache, unlike the segment records)
+	std::vector<uint64_t> gone((g.seg.size() + 63) / 64, 0);
+	for (size_t i = 0; i < g.seg.size(); ++i)
+		if (g.seg[i].del) gone[i >> 6] |= 1ULL << (i & 63);
+	auto is_gone = [&](uint32_t sid) { return (gone[sid >> 6] >> (sid & 63)) & 1; };
 	size_t n = 0;
 	for (size_t e = 0; e < g.arc.size(); ++e) {
 		const Arc &a = g.arc[e];
-		if (!a.del && !g.seg[a.head() >> 1].del && !g.seg[a.w >> 1].del) g.arc[n++] = a;
+		if (!a.del && !is_gone(a.head() >> 1) && !is_gone(a.w >> 1)) g.arc[n++] = a;
 	}
 	g.arc.resize(n);
 	bool sorted = true;
@@ -411,53 +490,27 @@ void finalize(Gfa &g) // gfa-base.c:455-466
 }
 
 // ---------------------------------------------------------------- reader (gfa-io.c:354-427)
-struct LineSource {
-	gzFile fp = nullptr;
+struct LineSource { // lines of an in-memory text, without their '\n' and one trailing '\r'
 	const char *mem = nullptr;
 	int64_t mem_len = 0, mem_pos = 0;
-	std::vector<char> buf;
-	int64_t bpos = 0, blen = 0;
-	bool eof = false;
 
-	bool getline(std::string &s)
+	bool getline(std::string_view &s)
 	{
-		s.clear();
-		bool any = false;
-		for (;;) {
-			const char *p, *e;
-			if (mem) {
-				if (mem_pos >= mem_len) break;
-				p = mem + mem_pos, e = mem + mem_len;
-			} else {
-				if (bpos >= blen) {
-					if (eof) break;
-					if (buf.empty()) buf.resize(1 << 16);
-					int r = gzread(fp, buf.data(), (unsigned)buf.size());
-					if (r <= 0) {
-						eof = true;
-						break;
-					}
-					blen = r, bpos = 0;
-				}
-				p = buf.data() + bpos, e = buf.data() + blen;
-			}
-			any = true;
-			const char *nl = (const char *)memchr(p, '\n', (size_t)(e - p));
-			const char *stop = nl ? nl : e;
-			s.append(p, (size_t)(stop - p));
-			const int64_t used = (int64_t)(stop - p) + (nl ? 1 : 0);
-			if (mem) mem_pos += used;
-			else bpos += used;
-			if (nl) break;
-		}
-		if (!s.empty() && s.back() == '\r') s.pop_back();
-		return any;
+		if (mem_pos >= mem_len) return false;
+		const char *p = mem + mem_pos, *e = mem + mem_len;
+		const char *nl = (const char *)memchr(p, '\n', (size_t)(e - p));
+		const char *stop = nl ? nl : e;
+		s = std::string_view(p, (size_t)(stop - p));
+		mem_pos += (int64_t)(stop - p) + (nl ? 1 : 0);
+		if (!s.empty() && s.back() == '\r') s.remove_suffix(1);
+		return true;
 	}
 };
 
 bool read_gfa(LineSource &src, Gfa &g)
 {
-	std::string s, fa_seq;
+	std::string_view s;
+	std::string fa_seq;
 	Fields fields;
 	bool is_fa = false;
 	int64_t fa_seg = -1;
@@ -491,6 +544,107 @@ bool read_gfa(LineSource &src, Gfa &g)
 		(void)ret; // the reference reports and skips invalid lines
 	}
 	if (is_fa) flush_fa();
+	finalize(g);
+	return true;
+}
+
+// ---------------------------------------------------------------- parallel parse
+// The text is cut at line ends into one chunk per thread. Each thread scans its chunk into S and
+// L records (fields, numbers, name hashes); the records are then applied on one thread in file
+// order, so segment ids (first appearance) and arc order are those of the sequential parse.
+// Name lookups are prefetched a few records ahead. Inputs with FASTA-style records ('>' lines)
+// go to the sequential parser.
+struct Chunk {
+	std::vector<uint8_t> kind; // 'S' or 'L', in line order
+	std::vector<SRec> s;
+	std::vector<LRec> l;
+	bool fasta = false;
+};
+
+void scan_chunk(const char *b, const char *e, Chunk &c)
+{
+	Fields f;
+	while (b < e) {
+		const char *nl = (const char *)memchr(b, '\n', (size_t)(e - b));
+		const char *le = nl ? nl : e;
+		std::string_view line(b, (size_t)(le - b));
+		b = nl ? nl + 1 : e;
+		if (!line.empty() && line.back() == '\r') line.remove_suffix(1);
+		if (!line.empty() && line[0] == '>') {
+			c.fasta = true;
+			return;
+		}
+		if (line.size() < 3 || line[1] != '\t') continue;
+		if (line[0] == 'S') {
+			SRec r;
+			if (scan_S(line, f, r)) c.s.push_back(r), c.kind.push_back('S');
+		} else if (line[0] == 'L') {
+			LRec r;
+			if (scan_L(line, f, r)) c.l.push_back(r), c.kind.push_back('L');
+		}
+	}
+}
+
+// Threads for a text of len bytes: GWF_GFA_THREADS if set, else one per core with at least
+// 1 MiB each, at most 16.
+int parse_threads(size_t len)
+{
+	if (const char *e = getenv("GWF_GFA_THREADS")) {
+		const int t = atoi(e);
+		return t < 1 ? 1 : (t > 64 ? 64 : t);
+	}
+	const unsigned hc = std::thread::hardware_concurrency();
+	size_t t = std::min<size_t>(hc ? hc : 1, 16);
+	t = std::min<size_t>(t, len >> 20);
+	return t < 1 ? 1 : (int)t;
+}
+
+// false: the caller parses sequentially
+bool read_gfa_parallel(const char *text, size_t len, Gfa &g)
+{
+	const int nt = parse_threads(len);
+	if (nt < 2) return false;
+	std::vector<const char *> cut((size_t)nt + 1);
+	cut[0] = text, cut[(size_t)nt] = text + len;
+	for (int t = 1; t < nt; ++t) {
+		const char *p = text + len * (size_t)t / (size_t)nt;
+		if (p < cut[(size_t)t - 1]) p = cut[(size_t)t - 1];
+		const char *nl = (const char *)memchr(p, '\n', (size_t)(text + len - p));
+		cut[(size_t)t] = nl ? nl + 1 : text + len;
+	}
+	std::vector<Chunk> ch((size_t)nt);
+	std::vector<std::thread> th;
+	for (int t = 1; t < nt; ++t) th.emplace_back(scan_chunk, cut[(size_t)t], cut[(size_t)t + 1], std::ref(ch[(size_t)t]));
+	scan_chunk(cut[0], cut[1], ch[0]);
+	for (auto &x : th) x.join();
+	size_t ns = 0, nl = 0, name_bytes = 0, seq_bytes = 0;
+	for (const Chunk &c : ch) {
+		if (c.fasta) return false;
+		ns += c.s.size(), nl += c.l.size();
+		for (const SRec &r : c.s) name_bytes += r.name.size(), seq_bytes += r.has_seq ? r.seq.size() : 0;
+	}
+	g.seg.reserve(ns + 16);
+	g.arc.reserve(2 * nl + 16);
+	g.seq_pool.reserve(seq_bytes + 16);
+	g.names.reserve(ns, name_bytes);
+	// slots kAhead records ahead, pool entries kNear records ahead
+	constexpr size_t kAhead = 16, kNear = 8;
+	for (const Chunk &c : ch) {
+		size_t is = 0, il = 0;
+		for (uint8_t k : c.kind) {
+			if (is + kAhead < c.s.size()) g.names.prefetch(c.s[is + kAhead].h);
+			if (il + kAhead < c.l.size()) {
+				g.names.prefetch(c.l[il + kAhead].hv);
+				g.names.prefetch(c.l[il + kAhead].hw);
+			}
+			if (il + kNear < c.l.size()) {
+				g.names.prefetch_entry(c.l[il + kNear].hv);
+				g.names.prefetch_entry(c.l[il + kNear].hw);
+			}
+			if (k == 'S') apply_S(g, c.s[is++]);
+			else apply_L(g, c.l[il++]);
+		}
+	}
 	finalize(g);
 	return true;
 }
@@ -678,10 +832,9 @@ gwf_graph_t *to_gwf(const Gfa &gfa, uint32_t v0) // main.cu:294-345
 	return g;
 }
 
-gwf_graph_t *load(LineSource &src, const char *start_seg)
+// The parsed graph from start_seg on, as a gwf_graph_t.
+gwf_graph_t *finish(Gfa &gfa, const char *start_seg)
 {
-	Gfa gfa;
-	read_gfa(src, gfa);
 	if (gfa.seg.empty()) {
 		gwf_set_error("GFA has no segments");
 		return nullptr;
@@ -707,18 +860,52 @@ gwf_graph_t *load(LineSource &src, const char *start_seg)
 	return to_gwf(gfa, v0);
 }
 
+gwf_graph_t *load_text(const char *text, size_t len, const char *start_seg)
+{
+	Gfa gfa;
+	if (!read_gfa_parallel(text, len, gfa)) {
+		gfa = Gfa();
+		LineSource src;
+		src.mem = text, src.mem_len = (int64_t)len;
+		read_gfa(src, gfa);
+	}
+	return finish(gfa, start_seg);
+}
+
 } // namespace
 
 extern "C" gwf_graph_t *gwf_gfa_load(const char *path, const char *start_seg)
 {
-	LineSource src;
-	src.fp = path && strcmp(path, "-") ? gzopen(path, "r") : gzdopen(0, "r");
-	if (!src.fp) {
+	gzFile fp = path && strcmp(path, "-") ? gzopen(path, "r") : gzdopen(0, "r");
+	if (!fp) {
 		gwf_set_error("cannot open GFA file");
 		return nullptr;
 	}
-	gwf_graph_t *g = load(src, start_seg);
-	gzclose(src.fp);
+	// the whole (decompressed) text in memory, then parsed in parallel; realloc grows the buffer
+	// without filling it
+	gzbuffer(fp, 1 << 20);
+	size_t cap = 1 << 24, n = 0;
+	char *text = (char *)malloc(cap);
+	for (; text;) {
+		if (cap - n < (1u << 22)) {
+			char *t2 = (char *)realloc(text, cap * 2);
+			if (!t2) {
+				free(text), text = nullptr;
+				break;
+			}
+			text = t2, cap *= 2;
+		}
+		const int r = gzread(fp, text + n, (unsigned)std::min<size_t>(cap - n, 1u << 30));
+		if (r <= 0) break;
+		n += (size_t)r;
+	}
+	gzclose(fp);
+	if (!text) {
+		gwf_set_error("out of host memory reading the GFA file");
+		return nullptr;
+	}
+	gwf_graph_t *g = load_text(text, n, start_seg);
+	free(text);
 	return g;
 }
 
@@ -728,9 +915,7 @@ extern "C" gwf_graph_t *gwf_gfa_load_mem(const char *text, int64_t len, const ch
 		gwf_set_error("null GFA text");
 		return nullptr;
 	}
-	LineSource src;
-	src.mem = text, src.mem_len = len;
-	return load(src, start_seg);
+	return load_text(text, (size_t)len, start_seg);
 }
 
 extern "C" void gwf_graph_free(gwf_graph_t *g)

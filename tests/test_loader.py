@@ -114,9 +114,11 @@ def _random_gfa(rng):
 
 
 @pytest.mark.skipif(not os.path.exists(REF_GWF_TEST), reason="reference gwf-test not built")
-def test_random_gfa_dumps_match_reference_binary(G, tmp_path):
+@pytest.mark.parametrize("threads", ["1", "3"])
+def test_random_gfa_dumps_match_reference_binary(G, tmp_path, monkeypatch, threads):
     """Random GFA texts through the reference's own loader (gwf-test -p, built from its sources) and
-    through the product loader: identical dumps."""
+    through the product loader, parsing on one thread and on three: identical dumps."""
+    monkeypatch.setenv("GWF_GFA_THREADS", threads)
     rng = np.random.default_rng(99)
     checked = 0
     for t in range(60):
@@ -134,3 +136,27 @@ def test_random_gfa_dumps_match_reference_binary(G, tmp_path):
         assert G.Graph.from_gfa(str(path)).dump() == ref.stdout, text.decode()
         checked += ref.stdout.count(b"S\t") > 3
     assert checked > 30
+
+
+@pytest.mark.skipif(not os.path.exists(REF_GWF_TEST), reason="reference gwf-test not built")
+def test_large_graph_parallel_parse_matches_reference(G, tmp_path, monkeypatch):
+    """A 2 Mbp graph (~100,000 segments): the parallel parse, the sequential parse and the
+    reference's gwf-test -p give the same dump."""
+    sg = G.SynthGraph(2_000_000, 50, 0.7, 20, 50_000, 1000, 5000, seed=9)
+    path = tmp_path / "g.gfa"
+    path.write_bytes(sg.gfa)
+    ref = subprocess.run([REF_GWF_TEST, "-p", str(path)], capture_output=True, timeout=120).stdout
+    monkeypatch.setenv("GWF_GFA_THREADS", "8")
+    par = G.Graph.from_gfa(str(path)).dump()
+    monkeypatch.setenv("GWF_GFA_THREADS", "1")
+    seq = G.Graph.from_gfa(str(path)).dump()
+    assert par == seq == ref and ref.count(b"\nS\t") > 50_000
+
+
+def test_gzip_input_equals_plain(G, tmp_path):
+    import gzip
+    src = os.path.join(GOLD, "graph_1000.gfa")
+    gz = tmp_path / "g.gfa.gz"
+    with gzip.open(gz, "wb") as f:
+        f.write(open(src, "rb").read())
+    assert G.Graph.from_gfa(str(gz)).dump() == G.Graph.from_gfa(src).dump()
