@@ -287,10 +287,12 @@ class Graph:
             raise GwfError(rc, last_error())
         return dist, st
 
-    def ed_path(self, reads, v0, v1=-1, flags=0, max_nv=4096):
+    def ed_path(self, reads, v0, v1=-1, flags=0, max_nv=4096, as_arrays=False):
         """Alignment with traceback (gwf_ed_batch_path). Returns (dist, status, end_off, paths),
         paths[i] = (vertices, arcs): the first min(path_n, max_nv) path vertices from v0 and the
-        index in the indexed graph's arcs of the arc into each (-1 for the first)."""
+        index in the indexed graph's arcs of the arc into each (-1 for the first). as_arrays=True
+        returns (dist, status, end_off, path_n, path_v, path_arc) with the n x max_nv rows as the
+        library wrote them."""
         cat, offs, lens = reads if isinstance(reads, tuple) else pack_reads(reads)
         n = len(lens)
         v0 = np.ascontiguousarray(np.broadcast_to(np.asarray(v0, dtype=np.int32), (n,)))
@@ -304,6 +306,8 @@ class Graph:
                                      _ptr(dist), _ptr(st), _ptr(end_off), _ptr(path_n), _ptr(pv), _ptr(pa))
         if rc != 0:
             raise GwfError(rc, last_error())
+        if as_arrays:
+            return dist, st, end_off, path_n, pv[:n], pa[:n]
         paths = [(pv[i, :min(path_n[i], max_nv)].copy(), pa[i, :min(path_n[i], max_nv)].copy()) for i in range(n)]
         return dist, st, end_off, paths
 

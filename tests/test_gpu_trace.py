@@ -116,6 +116,9 @@ def test_truncated_rows_and_failed_reads(G):
     assert np.array_equal(eo, eo2)
     for (fv, fa), (cv, ca) in zip(full, cut):
         assert np.array_equal(cv, fv[:2]) and np.array_equal(ca, fa[:2])
+    _, _, _, pn, pv, pa = g.ed_path(reads, w["v0"], max_nv=4096, as_arrays=True)
+    for i, (fv, fa) in enumerate(full):
+        assert pn[i] == len(fv) and np.array_equal(pv[i, :pn[i]], fv) and np.array_equal(pa[i, :pn[i]], fa)
     # an empty read is a per-read error: no path
     d, st, eo, paths = g.ed_path([b"", reads[0]], [0, int(w["v0"][0])])
     assert st[0] == G.GWF_E_BAD_INPUT and eo[0] == -1 and len(paths[0][0]) == 0
