@@ -95,7 +95,9 @@ void gwf_cleanup(gwf_graph_t *g);
 /* Host-callable single alignment. Replaces the device-only
  * gwf_ed(g, ql, q, v0, v1, max_lag, buf, diag_shared) of gwfa.h:95 with the upstream GWFA
  * signature. km is accepted and ignored (kalloc.c is empty in the reference). Synchronous.
- * Returns the edit distance, -1 if no alignment, or a GWF_E_* code. */
+ * max_lag is ignored as in the reference; traceback != 0 returns GWF_E_UNSUPPORTED (this signature
+ * has no path output: gwf_ed_batch_path returns paths). Returns the edit distance, -1 if no
+ * alignment, or a GWF_E_* code. */
 int32_t gwf_ed(void *km, const gwf_graph_t *g, int32_t ql, const char *q, int32_t v0, int32_t v1,
                uint32_t max_lag, int32_t traceback);
 
