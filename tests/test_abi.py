@@ -64,3 +64,22 @@ def test_synthetic_reads_are_deterministic(G):
     c = sg.reads(200, 1, 2000, 0.6, 500, 10000, 0.01, 0.10, seed=3)
     assert c["lens"].min() >= 450 and c["lens"].max() <= 10600
     assert 0.01 <= c["err"].min() and c["err"].max() <= 0.10
+
+
+def test_path_entry_point_arguments(G):
+    """gwf_ed_batch_path checks its arguments before it needs a device: negative counts, missing
+    output rows, an unindexed graph."""
+    g = G.Graph.from_gfa_text(b"S\ta\tACGT\n")
+    L = G.lib()
+    i32 = lambda n: np.zeros(n, dtype=np.int32)
+    cat = np.frombuffer(b"ACGT" + b"\0" * 16, dtype=np.uint8)
+    offs = np.zeros(1, dtype=np.int64)
+    lens, v0 = np.array([4], dtype=np.int32), i32(1)
+    d, st, eo, pn = i32(1), i32(1), i32(1), i32(1)
+    P = lambda a: a.ctypes.data
+    assert L.gwf_ed_batch_path(g.ptr, -1, P(cat), P(offs), P(lens), P(v0), -1, 0, 4, P(d), P(st), P(eo), P(pn),
+                               P(i32(4)), P(i32(4))) == G.GWF_E_BAD_INPUT
+    assert L.gwf_ed_batch_path(g.ptr, 1, P(cat), P(offs), P(lens), P(v0), -1, 0, 4, P(d), P(st), P(eo), P(pn),
+                               None, None) == G.GWF_E_BAD_INPUT
+    assert L.gwf_ed_batch_path(g.ptr, 1, P(cat), P(offs), P(lens), P(v0), -1, 0, 4, P(d), P(st), P(eo), P(pn),
+                               P(i32(4)), P(i32(4))) in (G.GWF_E_NOT_INDEXED, G.GWF_E_CUDA)
