@@ -32,7 +32,8 @@ OUT = os.path.join(ROOT, "gpurun_out", "golden")
 REF = "/root/reference"
 
 # synthetic sets: name -> (workload, n reads)
-SYNTH = {"config1": ("config1", 1000), "config2": ("config2", 2000), "config3": ("config3", 600)}
+SYNTH = {"config1": ("config1", 1000), "config2": ("config2", 2000), "config3": ("config3", 600),
+         "config4": ("config4", 200), "config5": ("config5", 100)}
 
 
 def pkg():

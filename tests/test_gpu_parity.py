@@ -28,7 +28,8 @@ def test_exposed_reads_match_reference(G, O):
         assert list(d) == ref
 
 
-@pytest.mark.parametrize("name,n", [("config1", 1000), ("config2", 2000), ("config3", 600)])
+@pytest.mark.parametrize("name,n", [("config1", 1000), ("config2", 2000), ("config3", 600), ("config4", 200),
+                                    ("config5", 100)])
 def test_synthetic_match_reference_and_oracle(G, O, name, n):
     idx, ref = read_golden("ref_%s.txt" % name)
     w = G.load_workload(name, n=n)

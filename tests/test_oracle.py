@@ -78,11 +78,13 @@ def test_oracle_matches_reference_on_exposed_reads(G, O):
     assert list(d) == ref
 
 
-@pytest.mark.parametrize("name", ["config1", "config2", "config3"])
+@pytest.mark.parametrize("name", ["config1", "config2", "config3", "config4", "config5"])
 def test_oracle_matches_reference_on_synthetic(G, O, name):
-    """Pins the oracle to the reference gwf_ed device routine run with per-read v0."""
+    """Pins the oracle to the reference gwf_ed device routine run with per-read v0 (configs 4
+    and 5: 10 kbp and up to 20 kbp reads on the 5 Mbp graph, the reads whose arena the
+    reference can hold)."""
     idx, ref = read_golden("ref_%s.txt" % name)
-    n = {"config1": 1000, "config2": 2000, "config3": 600}[name]
+    n = {"config1": 1000, "config2": 2000, "config3": 600, "config4": 200, "config5": 100}[name]
     w = G.load_workload(name, n=n)
     og = O.OracleGraph.from_graph(w["graph"])
     sel = np.array(idx)
