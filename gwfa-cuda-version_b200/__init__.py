@@ -76,6 +76,7 @@ SIGNATURES = {
     "gwf_ed_batch": (ctypes.c_int, [PG, I32, P, P, P, I32, U32, P, P, P]),
     "gwf_ed_batch_concat": (ctypes.c_int, [PG, I32, P, P, P, P, I32, U32, P, P, P]),
     "gwf_ed_batch_path": (ctypes.c_int, [PG, I32, P, P, P, P, I32, I32, I32, P, P, P, P, P, P]),
+    "gwf_ed_batch_align": (ctypes.c_int, [PG, I32, P, P, P, P, I32, I32, I32, I32, P, P, P, P, P, P, P, P]),
     "gwf_batch_create": (P, [PG, I32, P, P, P, P, I32, P]),
     "gwf_batch_run": (ctypes.c_int, [P, P, P]),
     "gwf_batch_results": (ctypes.c_int, [P, P, P]),
@@ -287,12 +288,14 @@ class Graph:
             raise GwfError(rc, last_error())
         return dist, st
 
-    def ed_path(self, reads, v0, v1=-1, flags=0, max_nv=4096, as_arrays=False):
-        """Alignment with traceback (gwf_ed_batch_path). Returns (dist, status, end_off, paths),
-        paths[i] = (vertices, arcs): the first min(path_n, max_nv) path vertices from v0 and the
-        index in the indexed graph's arcs of the arc into each (-1 for the first). as_arrays=True
-        returns (dist, status, end_off, path_n, path_v, path_arc) with the n x max_nv rows as the
-        library wrote them."""
+    def ed_path(self, reads, v0, v1=-1, flags=0, max_nv=4096, as_arrays=False, max_ops=0):
+        """Alignment with traceback (gwf_ed_batch_path; gwf_ed_batch_align when max_ops > 0).
+        Returns (dist, status, end_off, paths), paths[i] = (vertices, arcs): the first
+        min(path_n, max_nv) path vertices from v0 and the index in the indexed graph's arcs of the
+        arc into each (-1 for the first). With max_ops > 0 a fifth item, cigars[i]: the read's
+        CIGAR against its path text as a string ("12=1X3=2I..."), or None. as_arrays=True returns
+        (dist, status, end_off, path_n, path_v, path_arc[, cigar_n, cigar]) as the library wrote
+        them."""
         cat, offs, lens = reads if isinstance(reads, tuple) else pack_reads(reads)
         n = len(lens)
         v0 = np.ascontiguousarray(np.broadcast_to(np.asarray(v0, dtype=np.int32), (n,)))
@@ -302,14 +305,32 @@ class Graph:
         path_n = np.zeros(n, dtype=np.int32)
         pv = np.zeros((max(n, 1), max(max_nv, 1)), dtype=np.int32)
         pa = np.zeros((max(n, 1), max(max_nv, 1)), dtype=np.int32)
-        rc = lib().gwf_ed_batch_path(self.ptr, n, _ptr(cat), _ptr(offs), _ptr(lens), _ptr(v0), v1, flags, max_nv,
-                                     _ptr(dist), _ptr(st), _ptr(end_off), _ptr(path_n), _ptr(pv), _ptr(pa))
+        if max_ops > 0:
+            cn = np.zeros(n, dtype=np.int32)
+            cg = np.zeros((max(n, 1), max_ops), dtype=np.uint32)
+            rc = lib().gwf_ed_batch_align(self.ptr, n, _ptr(cat), _ptr(offs), _ptr(lens), _ptr(v0), v1, flags, max_nv,
+                                          max_ops, _ptr(dist), _ptr(st), _ptr(end_off), _ptr(path_n), _ptr(pv),
+                                          _ptr(pa), _ptr(cn), _ptr(cg))
+        else:
+            rc = lib().gwf_ed_batch_path(self.ptr, n, _ptr(cat), _ptr(offs), _ptr(lens), _ptr(v0), v1, flags, max_nv,
+                                         _ptr(dist), _ptr(st), _ptr(end_off), _ptr(path_n), _ptr(pv), _ptr(pa))
         if rc != 0:
             raise GwfError(rc, last_error())
         if as_arrays:
-            return dist, st, end_off, path_n, pv[:n], pa[:n]
+            out = (dist, st, end_off, path_n, pv[:n], pa[:n])
+            return out + ((cn, cg[:n]) if max_ops > 0 else ())
         paths = [(pv[i, :min(path_n[i], max_nv)].copy(), pa[i, :min(path_n[i], max_nv)].copy()) for i in range(n)]
-        return dist, st, end_off, paths
+        if max_ops <= 0:
+            return dist, st, end_off, paths
+        cigars = [cigar_string(cg[i, :cn[i]]) if 0 <= cn[i] <= max_ops else None for i in range(n)]
+        return dist, st, end_off, paths, cigars
+
+CIGAR_OPS = {0: "M", 1: "I", 2: "D", 7: "=", 8: "X"}
+
+
+def cigar_string(runs):
+    """BAM-coded runs (len << 4 | op) as a CIGAR string."""
+    return "".join("%d%s" % (int(x) >> 4, CIGAR_OPS[int(x) & 15]) for x in runs)
 
 
 TUNE_BUCKET_MAX = (1500, 3000, 6000, 12000, None)  # upper ql bound (exclusive) per bucket

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/gwfa.h"
+#include "gwf_cigar.cuh"
 #include "gwf_kernels.cuh"
 #include "gwf_runtime.h"
 #include "gwfa_internal.h"
@@ -796,8 +797,8 @@ extern "C" int32_t gwf_ed(void *km, const gwf_graph_t *g, int32_t ql, const char
 }
 
 // ------------------------------------------------------------------ traceback batches
-struct TraceBufs { // per-device path outputs of gwf_ed_batch_path
-	DBuf end_off, path_n, path_v, path_arc;
+struct TraceBufs { // per-device path and CIGAR outputs of gwf_ed_batch_align
+	DBuf end_off, path_n, path_v, path_arc, cigar_n, cigar, order, slot_off;
 };
 static std::unordered_map<int, TraceBufs *> g_trace_bufs;
 
@@ -844,14 +845,76 @@ static int launch_trace(Engine &E, KParams p, Batch &B, const std::vector<int32_
 	return 0;
 }
 
-extern "C" int gwf_ed_batch_path(const gwf_graph_t *g, int32_t n, const char *seqs, const int64_t *offs,
-                                 const int32_t *ql, const int32_t *v0, int32_t v1, int32_t flags,
-                                 int32_t max_nv, int32_t *dist, int32_t *status, int32_t *end_off,
-                                 int32_t *path_n, int32_t *path_v, int32_t *path_arc)
+// CIGAR launches over the reads whose path is complete: one warp per read, arenas sized from the
+// read's length and distance, in chunks that fit the budget. Reads whose wavefront table alone
+// would pass the budget (or 2 GiB) get cigar_n = -1.
+static int launch_cigar(Engine &E, const GraphDev &G, Batch &B, TraceBufs &T, const int32_t *h_dist,
+                        const int32_t *h_status, const int32_t *h_path_n, int32_t max_nv, int32_t max_ops,
+                        int *launches)
 {
-	if (n < 0 || max_nv < 0 ||
+	const int64_t budget = std::max<int64_t>(E.mem_budget, (int64_t)E.ws.cap);
+	const int64_t per_read_cap = std::min<int64_t>(budget, 2LL << 30);
+	std::vector<int32_t> ids;
+	for (int32_t r = 0; r < B.n; ++r) {
+		const bool want = h_status[r] == GWF_OK && h_dist[r] >= 0 && h_path_n[r] >= 1 && h_path_n[r] <= max_nv;
+		if (want && cigar_arena_bytes(B.h_ql[(size_t)r], h_dist[r]) <= per_read_cap) ids.push_back(r);
+	}
+	CK(cudaMemsetAsync(T.cigar_n.p, 0xff, 4 * (size_t)B.n, E.stream)); // -1 for the reads left out
+	CigarParams p;
+	memset(&p, 0, sizeof p);
+	p.g = G.view();
+	p.r = reads_view(B);
+	p.max_nv = max_nv, p.max_ops = max_ops;
+	p.dist = (const int32_t *)B.dist.p;
+	p.status = (const int32_t *)B.status.p;
+	p.end_off = (const int32_t *)T.end_off.p;
+	p.path_n = (const int32_t *)T.path_n.p;
+	p.path_v = (const int32_t *)T.path_v.p;
+	p.path_arc = (const int32_t *)T.path_arc.p;
+	p.cigar_n = (int32_t *)T.cigar_n.p;
+	p.cigar = (uint32_t *)T.cigar.p;
+	size_t start = 0;
+	std::vector<int64_t> offs;
+	while (start < ids.size()) {
+		offs.clear();
+		int64_t used = 0;
+		size_t end = start;
+		while (end < ids.size()) {
+			const int64_t sz = cigar_arena_bytes(B.h_ql[(size_t)ids[end]], h_dist[ids[end]]);
+			if (used + sz > budget && end > start) break;
+			offs.push_back(used);
+			used += sz;
+			++end;
+		}
+		int rc;
+		if ((rc = E.ws.ensure((size_t)std::max<int64_t>(used, 16)))) return rc;
+		if ((rc = T.slot_off.ensure(8 * offs.size()))) return rc;
+		if ((rc = T.order.ensure(4 * (end - start)))) return rc;
+		CK(cudaMemcpyAsync(T.slot_off.p, offs.data(), 8 * offs.size(), cudaMemcpyHostToDevice, E.stream));
+		CK(cudaMemcpyAsync(T.order.p, ids.data() + start, 4 * (end - start), cudaMemcpyHostToDevice, E.stream));
+		p.order = (const int32_t *)T.order.p;
+		p.n_order = (int32_t)(end - start);
+		p.ws = (uint8_t *)E.ws.p;
+		p.slot_off = (const int64_t *)T.slot_off.p;
+		const int ctas = (p.n_order + kWarpsPerCta - 1) / kWarpsPerCta;
+		k_cigar<<<ctas, 32 * kWarpsPerCta, 0, E.stream>>>(p);
+		CK(cudaGetLastError());
+		++*launches;
+		CK(cudaStreamSynchronize(E.stream)); // arenas and offsets are reused by the next chunk
+		start = end;
+	}
+	return 0;
+}
+
+extern "C" int gwf_ed_batch_align(const gwf_graph_t *g, int32_t n, const char *seqs, const int64_t *offs,
+                                  const int32_t *ql, const int32_t *v0, int32_t v1, int32_t flags,
+                                  int32_t max_nv, int32_t max_ops, int32_t *dist, int32_t *status,
+                                  int32_t *end_off, int32_t *path_n, int32_t *path_v, int32_t *path_arc,
+                                  int32_t *cigar_n, uint32_t *cigar)
+{
+	if (n < 0 || max_nv < 0 || max_ops < 0 ||
 	    (n > 0 && (!seqs || !offs || !ql || !v0 || !dist || !status || !end_off || !path_n ||
-	               (max_nv > 0 && (!path_v || !path_arc))))) {
+	               (max_nv > 0 && (!path_v || !path_arc)) || (max_ops > 0 && (!cigar_n || !cigar))))) {
 		gwf_set_error("bad batch arguments");
 		return GWF_E_BAD_INPUT;
 	}
@@ -870,9 +933,11 @@ extern "C" int gwf_ed_batch_path(const gwf_graph_t *g, int32_t n, const char *se
 	TraceBufs *&T = g_trace_bufs[E->device];
 	if (!T) T = new TraceBufs;
 	const size_t cells = (size_t)n * (size_t)std::max(max_nv, 1);
+	const size_t ops = (size_t)n * (size_t)std::max(max_ops, 1);
 	if ((rc = gwf_batch_load(*E, *B, n, seqs, offs, ql, v0, v1))) return rc;
 	if ((rc = T->end_off.ensure(4 * (size_t)n)) || (rc = T->path_n.ensure(4 * (size_t)n)) ||
 	    (rc = T->path_v.ensure(4 * cells)) || (rc = T->path_arc.ensure(4 * cells)) ||
+	    (max_ops > 0 && ((rc = T->cigar_n.ensure(4 * (size_t)n)) || (rc = T->cigar.ensure(4 * ops)))) ||
 	    (rc = E->retry_list.ensure(4 * (size_t)n + 4)) || (rc = E->retry_n.ensure(16)) ||
 	    (rc = E->h_small.ensure(4 * (size_t)n + 64)))
 		return rc;
@@ -908,7 +973,21 @@ extern "C" int gwf_ed_batch_path(const gwf_graph_t *g, int32_t n, const char *se
 		CK(cudaMemcpy(path_v, T->path_v.p, 4 * cells, cudaMemcpyDeviceToHost));
 		CK(cudaMemcpy(path_arc, T->path_arc.p, 4 * cells, cudaMemcpyDeviceToHost));
 	}
+	if (max_ops > 0) {
+		if ((rc = launch_cigar(*E, *G, *B, *T, dist, status, path_n, max_nv, max_ops, &launches))) return rc;
+		CK(cudaMemcpy(cigar_n, T->cigar_n.p, 4 * (size_t)n, cudaMemcpyDeviceToHost));
+		CK(cudaMemcpy(cigar, T->cigar.p, 4 * ops, cudaMemcpyDeviceToHost));
+	}
 	return 0;
+}
+
+extern "C" int gwf_ed_batch_path(const gwf_graph_t *g, int32_t n, const char *seqs, const int64_t *offs,
+                                 const int32_t *ql, const int32_t *v0, int32_t v1, int32_t flags,
+                                 int32_t max_nv, int32_t *dist, int32_t *status, int32_t *end_off,
+                                 int32_t *path_n, int32_t *path_v, int32_t *path_arc)
+{
+	return gwf_ed_batch_align(g, n, seqs, offs, ql, v0, v1, flags, max_nv, 0, dist, status, end_off, path_n,
+	                          path_v, path_arc, nullptr, nullptr);
 }
 
 // ------------------------------------------------------------------ resident batches

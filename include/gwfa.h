@@ -136,6 +136,20 @@ int gwf_ed_batch_path(const gwf_graph_t *g, int32_t n, const char *seqs, const i
                       int32_t *dist, int32_t *status, int32_t *end_off, int32_t *path_n,
                       int32_t *path_v, int32_t *path_arc);
 
+/* gwf_ed_batch_path plus the base-level alignment of each read against the text its path spells,
+ * as a CIGAR (no counterpart in the reference either). Row i of cigar (max_ops wide) holds
+ * cigar_n[i] runs len << 4 | op with the BAM codes 7 '=' (equal bases), 8 'X' (substitution),
+ * 1 'I' (a read base the path text lacks), 2 'D' (a path base the read lacks); only the first
+ * min(cigar_n[i], max_ops) are written. The CIGAR consumes the whole read and the whole text and
+ * is an optimal end-to-end alignment of the two: its cost (X + I + D) is at most dist[i], equal
+ * with GWF_F_EXACT_START and v1 = -1. cigar_n[i] = -1 when read i has no CIGAR: no alignment, a
+ * per-read error, a path longer than max_nv, or a wavefront table ((dist + 1)^2 int32) larger
+ * than 2 GiB or the memory budget. max_ops = 0 is gwf_ed_batch_path. */
+int gwf_ed_batch_align(const gwf_graph_t *g, int32_t n, const char *seqs, const int64_t *offs,
+                       const int32_t *ql, const int32_t *v0, int32_t v1, int32_t flags, int32_t max_nv,
+                       int32_t max_ops, int32_t *dist, int32_t *status, int32_t *end_off, int32_t *path_n,
+                       int32_t *path_v, int32_t *path_arc, int32_t *cigar_n, uint32_t *cigar);
+
 /* ---- device-resident batches (inputs uploaded once; used to time the kernel alone) ---- */
 typedef struct gwf_batch_s gwf_batch_t;
 gwf_batch_t *gwf_batch_create(const gwf_graph_t *g, int32_t n, const char *seqs,

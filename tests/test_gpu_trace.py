@@ -123,3 +123,91 @@ def test_truncated_rows_and_failed_reads(G):
     d, st, eo, paths = g.ed_path([b"", reads[0]], [0, int(w["v0"][0])])
     assert st[0] == G.GWF_E_BAD_INPUT and eo[0] == -1 and len(paths[0][0]) == 0
     assert st[1] == 0 and len(paths[1][0]) >= 1
+
+
+def check_cigar(q, text, runs, dist, exact):
+    """Walks the CIGAR over the read and the path text: every '=' base equal, every 'X' base
+    different, both sequences consumed; its cost is the optimal end-to-end distance of the two,
+    at most the traced distance (equal with the exact start state)."""
+    i = j = cost = 0
+    for x in runs:
+        n, op = int(x) >> 4, int(x) & 15
+        assert n > 0
+        if op == 7:
+            assert q[i:i + n] == text[j:j + n]
+            i, j = i + n, j + n
+        elif op == 8:
+            assert all(q[i + t] != text[j + t] for t in range(n))
+            i, j, cost = i + n, j + n, cost + n
+        elif op == 1:
+            i, cost = i + n, cost + n
+        elif op == 2:
+            j, cost = j + n, cost + n
+        else:
+            raise AssertionError("op %d" % op)
+    assert i == len(q) and j == len(text)
+    assert cost == edit_distance(q, text)
+    assert cost == dist if exact else cost <= dist
+    return cost
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_cigars_on_bubble_graph(G, exact):
+    w = G.load_workload("config2", n=200)
+    g = w["graph"]
+    g.index()
+    flags = G.GWF_F_EXACT_START if exact else 0
+    reads = _reads(w, 200)
+    d0, _ = g.ed_batch(reads, w["v0"], flags=flags)
+    d, st, eo, pn, pv, pa, cn, cg = g.ed_path(reads, w["v0"], flags=flags, max_ops=512, as_arrays=True)
+    assert np.array_equal(d, d0) and (st == 0).all() and (cn > 0).all()
+    seqs, arcs = g.seqs(), g.arcs()
+    for i in range(0, 200, 2):
+        text = path_text(g, seqs, arcs, pv[i, :pn[i]], pa[i, :pn[i]], eo[i])
+        check_cigar(reads[i], text, cg[i, :cn[i]], d[i], exact)
+    _, _, _, _, cigars = g.ed_path(reads[:3], w["v0"][:3], flags=flags, max_ops=512)
+    assert all(c and c[-1] in "=XID" for c in cigars)
+
+
+def test_cigars_on_random_graphs(G, O):
+    checked = 0
+    for t, (seqs_in, arcs_in, v0, v1, q) in enumerate(cases(818, 150, v1_prob=0.3)):
+        exact = bool(t & 1)
+        og = O.OracleGraph(seqs_in, arcs_in)
+        od, ost = og.ed(q, v0, v1, exact_start=exact)
+        if ost.flags & O.F_NONTERM:
+            continue
+        g = G.Graph.from_arrays(seqs_in, arcs_in)
+        g.index()
+        d, st, eo, pn, pv, pa, cn, cg = g.ed_path([q], [v0], v1=v1, flags=G.GWF_F_EXACT_START if exact else 0,
+                                                   max_ops=256, as_arrays=True)
+        assert st[0] == 0 and d[0] == od
+        if d[0] >= 0:
+            assert cn[0] > 0
+            text = path_text(g, g.seqs(), g.arcs(), pv[0, :pn[0]], pa[0, :pn[0]], eo[0])
+            check_cigar(q, text, cg[0, :cn[0]], d[0], exact and v1 < 0)
+        else:
+            assert cn[0] == -1
+        checked += 1
+        g.close()
+    assert checked > 100
+
+
+def test_cigars_on_long_reads(G):
+    w = G.load_workload("config5", n=12)
+    g = w["graph"]
+    g.index()
+    reads = _reads(w, 12)
+    d, st, eo, pn, pv, pa, cn, cg = g.ed_path(reads, w["v0"], flags=G.GWF_F_EXACT_START, max_ops=8192,
+                                               as_arrays=True)
+    assert (st == 0).all() and (cn > 0).all()
+    seqs, arcs = g.seqs(), g.arcs()
+    for i in range(12):
+        if len(reads[i]) > 6000:
+            continue  # the test's numpy DP is quadratic
+        text = path_text(g, seqs, arcs, pv[i, :pn[i]], pa[i, :pn[i]], eo[i])
+        check_cigar(reads[i], text, cg[i, :cn[i]], d[i], True)
+    # a row narrower than the CIGAR: the count is still the full count
+    _, _, _, _, _, _, cn2, cg2 = g.ed_path(reads[:2], w["v0"][:2], flags=G.GWF_F_EXACT_START, max_ops=4,
+                                           as_arrays=True)
+    assert np.array_equal(cn2, cn[:2]) and np.array_equal(cg2[:, :4], cg[:2, :4])
