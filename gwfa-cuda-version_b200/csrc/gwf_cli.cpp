@@ -10,8 +10,9 @@
 //   -P   apply -l: lag pruning (GWF_F_MAX_LAG; no reference counterpart); -t does not prune
 //   -m   execution form [persistent]
 //   -x   exact start state (GWF_F_EXACT_START)
-//   -t   traceback: after each distance, the end offset and the vertex path (no reference
-//        counterpart; the reference's traceback argument is unused, README.md:117-118)
+//   -t   traceback: after each distance, the end offset, the vertex path and the CIGAR of the
+//        read against the path's text (no reference counterpart; the reference's traceback
+//        argument is unused, README.md:117-118)
 //
 // Every read is aligned from offset 0 of the start segment (vertex 0 of the converted graph),
 // as the reference kernel does (main.cu:217). Timing and counts go to stderr.
@@ -81,7 +82,7 @@ void usage()
 	fprintf(stderr, "  -p        output GFA in the forward strand\n");
 	fprintf(stderr, "  -m STR    execution form: persistent or plain [persistent]\n");
 	fprintf(stderr, "  -x        exact start state (no reference start-state rule)\n");
-	fprintf(stderr, "  -t        traceback: print distance, end offset and vertex path per read\n");
+	fprintf(stderr, "  -t        traceback: print distance, end offset, vertex path and CIGAR per read\n");
 }
 
 } // namespace
@@ -152,21 +153,26 @@ int main(int argc, char *argv[])
 	std::vector<std::string> paths;
 	int rc = 0;
 	if (trace) {
-		// chunks of reads; a row of max_nv vertices, widened for a chunk whose paths are longer
+		// chunks of reads; rows of max_nv vertices and max_ops CIGAR runs, widened (one more
+		// pass) for a chunk whose paths or CIGARs are longer
 		paths.resize((size_t)n);
 		const int32_t chunk = 8192;
+		static const char kOp[16] = {'M', 'I', 'D', '?', '?', '?', '?', '=', 'X', '?', '?', '?', '?', '?', '?', '?'};
 		for (int32_t c0 = 0; c0 < n && !rc; c0 += chunk) {
 			const int32_t m = std::min(chunk, n - c0);
-			int32_t max_nv = 256;
-			std::vector<int32_t> eo((size_t)m), pn((size_t)m), pv, pa;
+			int32_t max_nv = 256, max_ops = 512;
+			std::vector<int32_t> eo((size_t)m), pn((size_t)m), cn((size_t)m), pv, pa;
+			std::vector<uint32_t> cg;
 			for (int pass = 0; pass < 2 && !rc; ++pass) {
 				pv.assign((size_t)m * (size_t)max_nv, 0), pa.assign((size_t)m * (size_t)max_nv, 0);
-				rc = gwf_ed_batch_path(g, m, cat.data(), offs.data() + c0, lens.data() + c0, v0.data() + c0, -1,
-				                       opt.flags, max_nv, dist.data() + c0, status.data() + c0, eo.data(), pn.data(),
-				                       pv.data(), pa.data());
-				const int32_t need = m ? *std::max_element(pn.begin(), pn.end()) : 0;
-				if (need <= max_nv) break;
-				max_nv = need;
+				cg.assign((size_t)m * (size_t)max_ops, 0);
+				rc = gwf_ed_batch_align(g, m, cat.data(), offs.data() + c0, lens.data() + c0, v0.data() + c0, -1,
+				                        opt.flags, max_nv, max_ops, dist.data() + c0, status.data() + c0, eo.data(),
+				                        pn.data(), pv.data(), pa.data(), cn.data(), cg.data());
+				const int32_t need_nv = m ? *std::max_element(pn.begin(), pn.end()) : 0;
+				const int32_t need_ops = m ? *std::max_element(cn.begin(), cn.end()) : 0;
+				if (need_nv <= max_nv && need_ops <= max_ops) break;
+				max_nv = std::max(max_nv, need_nv), max_ops = std::max(max_ops, need_ops);
 			}
 			for (int32_t j = 0; j < m && !rc; ++j) {
 				std::string &o = paths[(size_t)(c0 + j)];
@@ -174,6 +180,13 @@ int main(int argc, char *argv[])
 				for (int32_t k = 0; k < pn[(size_t)j] && k < max_nv; ++k) {
 					if (k) o += ',';
 					o += std::to_string(pv[(size_t)j * max_nv + k]);
+				}
+				o += '\t';
+				if (cn[(size_t)j] < 0 || cn[(size_t)j] > max_ops) o += '*';
+				for (int32_t k = 0; k >= 0 && k < cn[(size_t)j] && k < max_ops; ++k) {
+					const uint32_t x = cg[(size_t)j * max_ops + k];
+					o += std::to_string(x >> 4);
+					o += kOp[x & 15];
 				}
 			}
 		}

@@ -3,6 +3,7 @@ byte-identical to the reference's `gwf-test -p`, and on a GPU the reference's ow
 its exposed fixture (tolerance 0: int32 distances)."""
 import gzip
 import os
+import re
 import subprocess
 
 import numpy as np
@@ -63,21 +64,28 @@ def test_scores_equal_reference_gwf_test(form, tmp_path):
 @pytest.mark.gpu
 def test_traceback_option(G):
     """-t: the distance column equals the plain output; each path starts at vertex 0, follows arcs
-    of the converted graph, and ends at a valid offset of its last vertex."""
+    of the converted graph, and ends at a valid offset of its last vertex; each CIGAR consumes the
+    read and costs at most the distance."""
     gfa = os.path.join(GOLD, "graph_1000.gfa")
     reads = os.path.join(GOLD, "reads_200.fa")
     plain = run(gfa, reads).stdout.split()
     lines = run("-t", gfa, reads).stdout.splitlines()
+    reads_seq = [s for s in open(reads).read().split("\n") if s and not s.startswith(">")]
     assert [ln.split("\t")[0] for ln in lines] == plain
     g = G.Graph.from_gfa(gfa)
     g.index()
     arcs = {(v, w) for v, w, _ in g.arcs()}
     lens = g.lens()
-    for ln in lines:
-        d, eo, path = ln.split("\t")
+    assert len(lines) == len(reads_seq)
+    for ln, seq in zip(lines, reads_seq):
+        d, eo, path, cigar = ln.split("\t")
         verts = [int(x) for x in path.split(",")]
         assert verts[0] == 0 and all((a, b) in arcs for a, b in zip(verts, verts[1:]))
         assert 0 <= int(eo) < lens[verts[-1]]
+        ops = re.findall(r"(\d+)([=XID])", cigar)
+        assert "".join(n + o for n, o in ops) == cigar
+        assert sum(int(n) for n, o in ops if o in "=XI") == len(seq)
+        assert sum(int(n) for n, o in ops if o in "XID") <= int(d)
 
 
 @pytest.mark.gpu
