@@ -327,6 +327,9 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="persistent grid; 0 = occupancy limit")
     ap.add_argument("--graph", type=int, default=1, help="1 = persistent runs replay a captured CUDA graph")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--split", action="store_true",
+                    help="strong scaling: every rank holds the same workload, aligns its cost-balanced "
+                         "range (partition_reads) and the distances are all-gathered")
     ap.add_argument("--reads", type=int, default=0,
                     help="the first N reads of the workload (small profiling cases); 0 = all")
     ap.add_argument("--serving", action="store_true", help="serving benchmark (config5) instead")
@@ -360,12 +363,19 @@ def main():
     torch.cuda.set_device(local)
     G = pkg()
     mode = G.MODE_PERSISTENT if args.mode == "persistent" else G.MODE_PLAIN
-    w = G.load_workload(args.workload, n=args.reads or None, seed=shard_seed(args.workload, rank), pinned=True)
+    seed = None if args.split else shard_seed(args.workload, rank)
+    w = G.load_workload(args.workload, n=args.reads or None, seed=seed, pinned=True)
     g = w["graph"]
     g.index()
-    n = len(w["lens"])
-    bases = float(np.sum(w["lens"]))
-    batch = G.ResidentBatch(g, w["cat"], w["offs"], w["lens"], w["v0"], mode=mode)
+    n_total = len(w["lens"])
+    # weak scaling: this rank's own workload; --split: this rank's range of the shared workload
+    lo, hi = G.partition_reads(w["lens"], world)[rank] if args.split else (0, n_total)
+    r_offs, r_lens, r_v0 = (np.ascontiguousarray(w[k][lo:hi]) for k in ("offs", "lens", "v0"))
+    n = hi - lo
+    bases = float(np.sum(r_lens))
+    job_reads = n_total if args.split else world * n
+    job_bases = float(np.sum(w["lens"])) if args.split else world * bases
+    batch = G.ResidentBatch(g, w["cat"], r_offs, r_lens, r_v0, mode=mode)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
     def barrier():
@@ -392,7 +402,7 @@ def main():
         torch.cuda.synchronize()
     barrier()
     ms = max_over_ranks(statistics.mean(times))
-    value = world * n / (ms / 1000.0)
+    value = job_reads / (ms / 1000.0)
 
     # the other form on the same reads, for the persistent-vs-plain comparison
     forms = {}
@@ -412,28 +422,38 @@ def main():
 
     # end to end through the public batch call, pinned host buffers, copies in the timed region
     e2e_t = []
+    dist_full = None  # --split: every read's distance, gathered from all ranks
     if not args.no_e2e:
-        for _ in range(2):
+        def e2e_call():
+            if args.split:
+                return G.align_sharded(g, (w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode)[0]
             g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode)
+        for _ in range(2):
+            e2e_call()
         barrier()
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode)
+            dist_full = e2e_call()
             e2e_t.append(time.perf_counter() - t0)
         barrier()
     e2e_s = max_over_ranks(statistics.mean(e2e_t)) if e2e_t else None
-    h2d = int(w["offs"][-1] + w["lens"][-1]) + n * (8 + 4 + 4 + 8 + 4)
-    d2h = n * 8 + 4
+    # bytes of the whole job per step: read bytes plus per-read offsets, lengths, v0 and queue
+    # metadata in, distance and status out
+    h2d = int(job_bases) + job_reads * (8 + 4 + 4 + 8 + 4)
+    d2h = job_reads * 8 + 4
 
     line = {
         "metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong" if args.split else "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "config": {"workload": WORKLOAD_DESC[args.workload], "reads_per_gpu": n, "form": args.mode,
                    "cuda_graph": bool(use_graph),
-                   "l2": "flushed between steps (256 MB write)", "parallelism": "reads sharded by rank, graph replicated"},
-        "gbases_per_s": world * bases / (ms / 1000.0) / 1e9,
-        "e2e": ({"value": world * n / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+                   "l2": "flushed between steps (256 MB write)",
+                   "parallelism": ("one batch split by cost over the ranks, distances all-gathered, graph replicated"
+                                   if args.split else "reads sharded by rank, graph replicated")},
+        "gbases_per_s": job_bases / (ms / 1000.0) / 1e9,
+        "e2e": ({"value": job_reads / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
                 if e2e_s else None),
         "gpu_launches": launches,
         "status_ok": bool((status == 0).all()),
@@ -445,8 +465,13 @@ def main():
     if rank == 0 and not args.no_cpu:
         cpu = cpu_oracle_run(w)
         sel = cpu["sel"]
-        line["bit_exact_vs_oracle"] = {"reads_checked": int(len(sel)),
-                                       "mismatches": int(np.sum(cpu["dist"] != dist_gpu[sel]))}
+        if args.split and dist_full is not None:
+            chk, got = np.ones(len(sel), dtype=bool), dist_full[sel]
+        else:  # this rank's reads
+            chk = (sel >= lo) & (sel < hi)
+            got = dist_gpu[sel[chk] - lo]
+        line["bit_exact_vs_oracle"] = {"reads_checked": int(chk.sum()),
+                                       "mismatches": int(np.sum(cpu["dist"][chk] != got))}
         line["cpu_baseline"] = {"value": len(sel) / cpu["seconds"], "unit": "reads/s", "cores": cpu["threads"],
                                 "kind": "port",
                                 "sample": ("whole workload" if cpu["full"] else "%d evenly spread reads" % len(sel))

@@ -325,6 +325,59 @@ class Graph:
         cigars = [cigar_string(cg[i, :cn[i]]) if 0 <= cn[i] <= max_ops else None for i in range(n)]
         return dist, st, end_off, paths, cigars
 
+# ---- one batch over several GPUs (one process per GPU, torch.distributed)
+def partition_reads(lens, world, cost=None):
+    """Cost-balanced split of a batch into `world` contiguous ranges of reads: the boundaries cut
+    the running sum of the per-read cost (default ql^2, the work of a read grows with its length
+    times its score) into equal parts. Contiguous ranges keep each rank's upload to its own
+    bytes; inside a range the persistent queue orders the reads longest first. Returns
+    [(start, end)] per rank."""
+    lens = np.asarray(lens)
+    n = len(lens)
+    c = (lens.astype(np.float64) ** 2) if cost is None else np.asarray(cost, dtype=np.float64)
+    cum = np.cumsum(c)
+    total = float(cum[-1]) if n else 0.0
+    cuts = [0] + [int(np.searchsorted(cum, total * k / world, side="left")) + 1 for k in range(1, world)] + [n]
+    cuts = np.minimum(np.maximum.accumulate(np.array(cuts)), n)
+    return [(int(cuts[k]), int(cuts[k + 1])) for k in range(world)]
+
+
+def align_sharded(graph, reads, v0, v1=-1, mode=MODE_AUTO, flags=0, group=None, align_fn=None):
+    """Aligns a batch that every rank holds, split across the ranks of torch.distributed's default
+    group (or `group`) by partition_reads: each rank aligns its range on its own GPU, then the
+    int32 distances and statuses are all-gathered (NCCL over NVLink with CUDA tensors, gloo on
+    CPU), so every rank returns the full (dist, status). The graph is replicated: every rank has
+    indexed its own copy. Without an initialised process group this is graph.ed_batch.
+    align_fn(cat, offs, lens, v0) -> (dist, status) stands in for graph.ed_batch (tests)."""
+    cat, offs, lens = reads if isinstance(reads, tuple) else pack_reads(reads)
+    n = len(lens)
+    v0 = np.ascontiguousarray(np.broadcast_to(np.asarray(v0, dtype=np.int32), (n,)))
+    run = align_fn or (lambda c, o, l, v: graph.ed_batch((c, o, l), v, v1=v1, mode=mode, flags=flags))
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return run(cat, offs, lens, v0)
+    import torch
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    parts = partition_reads(lens, world)
+    a, b = parts[rank]
+    d, st = run(cat, np.ascontiguousarray(offs[a:b]), np.ascontiguousarray(lens[a:b]), np.ascontiguousarray(v0[a:b]))
+    width = max(1, max(e - s for s, e in parts))
+    device = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    buf = torch.full((2, width), -1, dtype=torch.int32)
+    buf[0, :b - a] = torch.from_numpy(np.asarray(d, dtype=np.int32))
+    buf[1, :b - a] = torch.from_numpy(np.asarray(st, dtype=np.int32))
+    buf = buf.to(device)
+    out = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(out, buf, group=group)
+    dist_all = np.empty(n, dtype=np.int32)
+    st_all = np.empty(n, dtype=np.int32)
+    for r, (s0, e0) in enumerate(parts):
+        x = out[r].cpu().numpy()
+        dist_all[s0:e0] = x[0, :e0 - s0]
+        st_all[s0:e0] = x[1, :e0 - s0]
+    return dist_all, st_all
+
+
 CIGAR_OPS = {0: "M", 1: "I", 2: "D", 7: "=", 8: "X"}
 
 

@@ -79,3 +79,65 @@ def test_rank0_shard_is_the_published_workload(G):
     b = G.load_workload("config1", n=30)
     assert np.array_equal(a["cat"], b["cat"]) and np.array_equal(a["v0"], b["v0"])
     assert bench.reduce_max(1.5) == 1.5
+
+
+def _split_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        import bench
+        G = bench.pkg()
+        rng = np.random.default_rng(7)  # the same batch on every rank
+        reads = [bytes(rng.choice(list(b"ACGT"), size=int(rng.integers(50, 400))).astype(np.uint8)) for _ in range(101)]
+        v0 = rng.integers(0, 9, 101).astype(np.int32)
+        seen = []
+
+        def fake(cat, offs, lens, vv):  # stands in for the GPU: a function of the read's bytes
+            seen.append(len(lens))
+            d = np.array([int(cat[o:o + l].astype(np.int64).sum()) % 1000 + int(x) for o, l, x in zip(offs, lens, vv)],
+                         dtype=np.int32)
+            return d, np.full(len(lens), rank, dtype=np.int32)
+
+        d, st = G.align_sharded(None, reads, v0, align_fn=fake)
+        q.put((rank, d.tolist(), st.tolist(), seen))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_split_batch_over_two_gloo_ranks(G):
+    """align_sharded: one batch split by cost over two ranks, each rank aligns only its range,
+    and the all-gather gives both ranks the full results in input order."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_split_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = {}
+    for _ in procs:
+        rank, d, st, seen = q.get(timeout=240)
+        out[rank] = (d, st, seen)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    rng = np.random.default_rng(7)
+    reads = [bytes(rng.choice(list(b"ACGT"), size=int(rng.integers(50, 400))).astype(np.uint8)) for _ in range(101)]
+    v0 = rng.integers(0, 9, 101).astype(np.int32)
+    want = [sum(r) % 1000 + int(x) for r, x in zip(reads, v0)]
+    parts = G.partition_reads([len(r) for r in reads], 2)
+    assert out[0][0] == out[1][0] == want
+    assert out[0][1] == out[1][1] == [0] * parts[0][1] + [1] * (101 - parts[0][1])
+    assert out[0][2] == [parts[0][1] - parts[0][0]] and out[1][2] == [parts[1][1] - parts[1][0]]
+
+
+def test_partition_is_contiguous_and_balanced(G):
+    rng = np.random.default_rng(3)
+    lens = rng.integers(500, 10000, 5000)
+    for world in (1, 2, 4, 8):
+        parts = G.partition_reads(lens, world)
+        assert parts[0][0] == 0 and parts[-1][1] == len(lens)
+        assert all(parts[k][1] == parts[k + 1][0] for k in range(world - 1))
+        loads = [float((lens[a:b].astype(float) ** 2).sum()) for a, b in parts]
+        assert max(loads) <= 1.02 * sum(loads) / world
