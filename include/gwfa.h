@@ -247,7 +247,10 @@ void gwf_srv_destroy(gwf_srv_t *s);
 /* gfa_read + gfa_finalize + gwf_gfa2gwf in one call. start_seg = segment name of v0 on the
  * forward strand (main.cu:399-407), or the name followed by '+' or '-' to choose the strand
  * (the reference leaves that as a TODO, main.cu:404); NULL = first segment, forward. Vertex 0
- * of the result is the start segment on that strand. Returns NULL on failure. */
+ * of the result is the start segment on that strand. Returns NULL on failure. path may be
+ * gzip-compressed, or "-" for standard input. The text is parsed on one thread per core (at
+ * least 1 MiB each; the environment variable GWF_GFA_THREADS sets the count) and applied in file
+ * order, so the result does not depend on the thread count. */
 gwf_graph_t *gwf_gfa_load(const char *path, const char *start_seg);
 /* Same from an in-memory GFA text. */
 gwf_graph_t *gwf_gfa_load_mem(const char *text, int64_t len, const char *start_seg);
