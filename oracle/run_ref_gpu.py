@@ -5,7 +5,7 @@ per-read v0) on the benchmark workloads, on the same GPU.
 Reads that the oracle flags as unsafe for the reference (arena overflow, non-termination) are
 left out so the reference is never given an input that can fault or hang; the count is reported.
 
-    python oracle/run_ref_gpu.py config2 [config1 config3 config4] > gpurun_out/ref_gpu.json
+    python oracle/run_ref_gpu.py config2 [config1 config3 config4] > ref_gpu.json
     python oracle/run_ref_gpu.py config4:2000      # the first 2,000 reads of a workload
 """
 import importlib.util

@@ -7,14 +7,14 @@ Stages (run in order):
             synthetic read sets to _work/golden_inputs/ as FASTA + per-read v0. Reads that the
             oracle flags as unsafe for the reference (arena overflow, non-termination) are
             left out, so the reference kernel is never given an input that can fault or hang.
-  run       (GPU box): runs oracle/_ref/gwf-test and oracle/_ref/gwf-ref-harness (the
-            reference's own CUDA code, built by `make -C oracle ref`) on those inputs; writes
-            gpurun_out/golden/*.txt.
-  collect   (CPU): copies the reference outputs into tests/golden/ref_*.txt.
+  run       (a machine with a B200): runs oracle/_ref/gwf-test and oracle/_ref/gwf-ref-harness
+            (the reference's own CUDA code, built by `make -C oracle ref`) on those inputs;
+            writes OUTDIR/*.txt.
+  collect   (CPU): copies the reference outputs from OUTDIR into tests/golden/ref_*.txt.
 
     python tests/golden/make_golden.py prepare
-    python tests/golden/make_golden.py run        # under gpurun
-    python tests/golden/make_golden.py collect
+    python tests/golden/make_golden.py run OUTDIR       # on the GPU machine
+    python tests/golden/make_golden.py collect OUTDIR   # OUTDIR brought back here
 """
 import importlib.util
 import json
@@ -28,7 +28,7 @@ import numpy as np
 ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
 GOLD = os.path.join(ROOT, "tests", "golden")
 INP = os.path.join(ROOT, "_work", "golden_inputs")
-OUT = os.path.join(ROOT, "gpurun_out", "golden")
+OUT = None  # the reference outputs' directory, from the command line
 REF = "/root/reference"
 
 # synthetic sets: name -> (workload, n reads)
@@ -147,4 +147,6 @@ def collect():
 
 
 if __name__ == "__main__":
+    if sys.argv[1] in ("run", "collect"):
+        OUT = os.path.abspath(sys.argv[2])
     {"prepare": prepare, "run": run, "collect": collect}[sys.argv[1]]()
