@@ -63,6 +63,11 @@ class SrvOpts(ctypes.Structure):
                 ("flags", ctypes.c_int32), ("device", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7)]
 
 
+class GwfReads(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("n_bases", ctypes.c_int64), ("seqs", ctypes.c_void_p),
+                ("offs", ctypes.POINTER(ctypes.c_int64)), ("lens", ctypes.POINTER(ctypes.c_int32))]
+
+
 _lib = None
 P = ctypes.c_void_p
 I32, I64, U32, U64, DBL = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double
@@ -76,6 +81,8 @@ SIGNATURES = {
     "gwf_ed_batch": (ctypes.c_int, [PG, I32, P, P, P, I32, U32, P, P, P]),
     "gwf_ed_batch_concat": (ctypes.c_int, [PG, I32, P, P, P, P, I32, U32, P, P, P]),
     "gwf_ed_batch_path": (ctypes.c_int, [PG, I32, P, P, P, P, I32, I32, I32, P, P, P, P, P, P]),
+    "gwf_reads_load": (ctypes.POINTER(GwfReads), [ctypes.c_char_p]),
+    "gwf_reads_free": (None, [ctypes.POINTER(GwfReads)]),
     "gwf_ed_batch_align": (ctypes.c_int, [PG, I32, P, P, P, P, I32, I32, I32, I32, P, P, P, P, P, P, P, P]),
     "gwf_batch_create": (P, [PG, I32, P, P, P, P, I32, P]),
     "gwf_batch_run": (ctypes.c_int, [P, P, P]),
@@ -140,6 +147,22 @@ def last_error():
 
 def _ptr(a):
     return a.ctypes.data if a is not None else None
+
+
+def load_reads(path):
+    """gwf_reads_load: a FASTA/FASTQ file (plain or gzip) as (cat, offs, lens) numpy copies, the
+    layout ed_batch takes."""
+    r = lib().gwf_reads_load(path.encode())
+    if not r:
+        raise GwfError(GWF_E_BAD_INPUT, last_error())
+    try:
+        n, nb = r.contents.n, r.contents.n_bases
+        cat = np.frombuffer(ctypes.string_at(r.contents.seqs, nb + 16), dtype=np.uint8).copy()
+        offs = np.ctypeslib.as_array(r.contents.offs, shape=(max(n, 1),))[:n].copy()
+        lens = np.ctypeslib.as_array(r.contents.lens, shape=(max(n, 1),))[:n].copy()
+    finally:
+        lib().gwf_reads_free(r)
+    return cat, offs, lens
 
 
 def pack_reads(reads):

@@ -12,7 +12,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgwfa_b200.so")
 CLI = os.path.join(HERE, "gwf-b200")
-SOURCES = ["gwf_runtime.cu", "gwf_serve.cu", "gwf_tune.cu", "gwf_noalloc.cu", "gfa_loader.cpp", "synth.cpp"]
+SOURCES = ["gwf_runtime.cu", "gwf_serve.cu", "gwf_tune.cu", "gwf_noalloc.cu", "gfa_loader.cpp", "reads_loader.cpp",
+           "synth.cpp"]
 # gwf_cli.cpp is the command-line driver (a separate executable, not part of the library)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -874,15 +874,15 @@ gwf_graph_t *load_text(const char *text, size_t len, const char *start_seg)
 
 } // namespace
 
-extern "C" gwf_graph_t *gwf_gfa_load(const char *path, const char *start_seg)
+// The whole (decompressed) file in one malloc'd buffer; realloc grows it without filling it.
+// "-" or NULL is standard input. Returns NULL (and sets the error) on failure.
+char *gwf_read_file(const char *path, size_t *len)
 {
 	gzFile fp = path && strcmp(path, "-") ? gzopen(path, "r") : gzdopen(0, "r");
 	if (!fp) {
-		gwf_set_error("cannot open GFA file");
+		gwf_set_error("cannot open input file");
 		return nullptr;
 	}
-	// the whole (decompressed) text in memory, then parsed in parallel; realloc grows the buffer
-	// without filling it
 	gzbuffer(fp, 1 << 20);
 	size_t cap = 1 << 24, n = 0;
 	char *text = (char *)malloc(cap);
@@ -901,9 +901,18 @@ extern "C" gwf_graph_t *gwf_gfa_load(const char *path, const char *start_seg)
 	}
 	gzclose(fp);
 	if (!text) {
-		gwf_set_error("out of host memory reading the GFA file");
+		gwf_set_error("out of host memory reading the input file");
 		return nullptr;
 	}
+	*len = n;
+	return text;
+}
+
+extern "C" gwf_graph_t *gwf_gfa_load(const char *path, const char *start_seg)
+{
+	size_t n = 0;
+	char *text = gwf_read_file(path, &n);
+	if (!text) return nullptr;
 	gwf_graph_t *g = load_text(text, n, start_seg);
 	free(text);
 	return g;

@@ -16,8 +16,6 @@
 //
 // Every read is aligned from offset 0 of the start segment (vertex 0 of the converted graph),
 // as the reference kernel does (main.cu:217). Timing and counts go to stderr.
-#include <zlib.h>
-
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -29,48 +27,6 @@
 #include "../../include/gwfa.h"
 
 namespace {
-
-// FASTA/FASTQ records, plain or gzip, sequences concatenated (multi-line FASTA joined).
-bool read_seqs(const char *path, std::vector<char> &cat, std::vector<int64_t> &offs, std::vector<int32_t> &lens)
-{
-	gzFile fp = gzopen(path, "r");
-	if (!fp) return false;
-	std::vector<char> line(1 << 16);
-	std::string cur;
-	bool in_seq = false, fastq = false;
-	int fq_state = 0; // 0 header, 1 sequence, 2 plus line, 3 qualities
-	auto flush = [&]() {
-		if (!in_seq) return;
-		offs.push_back((int64_t)cat.size());
-		lens.push_back((int32_t)cur.size());
-		cat.insert(cat.end(), cur.begin(), cur.end());
-		cur.clear();
-		in_seq = false;
-	};
-	std::string buf;
-	while (gzgets(fp, line.data(), (int)line.size())) {
-		buf.append(line.data());
-		if (buf.empty() || (buf.back() != '\n' && !gzeof(fp))) continue; // long line: keep reading
-		while (!buf.empty() && (buf.back() == '\n' || buf.back() == '\r')) buf.pop_back();
-		if (fastq) {
-			if (fq_state == 0 && !buf.empty() && buf[0] == '@') fq_state = 1, in_seq = true;
-			else if (fq_state == 1) cur = buf, fq_state = 2;
-			else if (fq_state == 2) flush(), fq_state = 3;
-			else if (fq_state == 3) fq_state = 0;
-		} else if (!buf.empty() && buf[0] == '>') {
-			flush();
-			in_seq = true;
-		} else if (!buf.empty() && buf[0] == '@' && offs.empty() && !in_seq) {
-			fastq = true, fq_state = 1, in_seq = true;
-		} else if (in_seq) {
-			cur += buf;
-		}
-		buf.clear();
-	}
-	if (!fastq) flush();
-	gzclose(fp);
-	return true;
-}
 
 void usage()
 {
@@ -132,17 +88,19 @@ int main(int argc, char *argv[])
 		gwf_graph_free(g);
 		return 0;
 	}
-	std::vector<char> cat;
-	std::vector<int64_t> offs;
-	std::vector<int32_t> lens;
-	if (!read_seqs(argv[i + 1], cat, offs, lens)) {
-		fprintf(stderr, "ERROR: cannot read %s\n", argv[i + 1]);
+	// the reads, concatenated, through the library's reader (FASTA/FASTQ, plain or gzip)
+	gwf_reads_t *rs = gwf_reads_load(argv[i + 1]);
+	if (!rs) {
+		fprintf(stderr, "ERROR: cannot read %s: %s\n", argv[i + 1], gwf_last_error());
 		gwf_graph_free(g);
 		return 1;
 	}
-	cat.resize(cat.size() + 16, 0);
-	const int32_t n = (int32_t)lens.size();
-	fprintf(stderr, "[gwf-b200] %d reads, %zu bases, %u vertices, %u arcs\n", n, cat.size() - 16, g->n_vtx, g->n_arc);
+	const char *cat = rs->seqs;
+	const std::vector<int64_t> offs(rs->offs, rs->offs + rs->n);
+	const std::vector<int32_t> lens(rs->lens, rs->lens + rs->n);
+	const int32_t n = rs->n;
+	fprintf(stderr, "[gwf-b200] %d reads, %lld bases, %u vertices, %u arcs\n", n, (long long)rs->n_bases, g->n_vtx,
+	        g->n_arc);
 	gwf_ed_index(g);
 	std::vector<int32_t> v0((size_t)n, 0), dist((size_t)n, -1), status((size_t)n, 0);
 	gwf_batch_opts_t opt;
@@ -166,7 +124,7 @@ int main(int argc, char *argv[])
 			for (int pass = 0; pass < 2 && !rc; ++pass) {
 				pv.assign((size_t)m * (size_t)max_nv, 0), pa.assign((size_t)m * (size_t)max_nv, 0);
 				cg.assign((size_t)m * (size_t)max_ops, 0);
-				rc = gwf_ed_batch_align(g, m, cat.data(), offs.data() + c0, lens.data() + c0, v0.data() + c0, -1,
+				rc = gwf_ed_batch_align(g, m, cat, offs.data() + c0, lens.data() + c0, v0.data() + c0, -1,
 				                        opt.flags, max_nv, max_ops, dist.data() + c0, status.data() + c0, eo.data(),
 				                        pn.data(), pv.data(), pa.data(), cn.data(), cg.data());
 				const int32_t need_nv = m ? *std::max_element(pn.begin(), pn.end()) : 0;
@@ -191,12 +149,13 @@ int main(int argc, char *argv[])
 			}
 		}
 	} else if (n > 0) {
-		rc = gwf_ed_batch_concat(g, n, cat.data(), offs.data(), lens.data(), v0.data(), -1, max_lag, dist.data(),
+		rc = gwf_ed_batch_concat(g, n, cat, offs.data(), lens.data(), v0.data(), -1, max_lag, dist.data(),
 		                         status.data(), &opt);
 	}
 	const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 	if (rc) {
 		fprintf(stderr, "ERROR: batch alignment failed (%d): %s\n", rc, gwf_last_error());
+		gwf_reads_free(rs);
 		gwf_graph_free(g);
 		return 1;
 	}
@@ -207,6 +166,7 @@ int main(int argc, char *argv[])
 		if (status[(size_t)j] != GWF_OK) ++bad;
 	}
 	fprintf(stderr, "[gwf-b200] aligned in %.6f s (%d reads with a per-read error status)\n", el, bad);
+	gwf_reads_free(rs);
 	gwf_graph_free(g);
 	return bad ? 2 : 0;
 }

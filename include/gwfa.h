@@ -260,6 +260,22 @@ void gwf_graph_free(gwf_graph_t *g);
  * most cap bytes (NUL-terminated when it fits). */
 int64_t gwf_graph_dump(const gwf_graph_t *g, char *buf, int64_t cap);
 
+/* ---- read sets (replaces the reference's two-pass FASTA reading, main.cu:459-534) ----
+ * FASTA or FASTQ (four-line records), plain or gzip, "-" = standard input. The sequences are
+ * concatenated in file order into seqs (16 zero bytes after the last), read i being
+ * seqs[offs[i] .. offs[i] + lens[i]), ready for gwf_ed_batch_concat. FASTA is parsed on one
+ * thread per core (at least 4 MiB each; GWF_READS_THREADS sets the count). Returns NULL on
+ * failure; free with gwf_reads_free. */
+typedef struct {
+	int32_t n;
+	int64_t n_bases;
+	char *seqs;
+	int64_t *offs;
+	int32_t *lens;
+} gwf_reads_t;
+gwf_reads_t *gwf_reads_load(const char *path);
+void gwf_reads_free(gwf_reads_t *r);
+
 /* ---- diagnostics ---- */
 const char *gwf_last_error(void);
 const char *gwf_version(void);
