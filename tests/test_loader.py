@@ -160,3 +160,12 @@ def test_gzip_input_equals_plain(G, tmp_path):
     with gzip.open(gz, "wb") as f:
         f.write(open(src, "rb").read())
     assert G.Graph.from_gfa(str(gz)).dump() == G.Graph.from_gfa(src).dump()
+
+
+def test_segment_without_sequence_becomes_n(G):
+    """An S line with '*' and an LN tag: the reference's conversion reads a null sequence there
+    (it crashes); this loader spells the segment as N bases and records an error message."""
+    text = b"S\ta\tACGT\nS\tb\t*\tLN:i:5\nS\tc\tGG\nL\ta\t+\tb\t+\t0M\nL\tb\t+\tc\t+\t0M\n"
+    g = G.Graph.from_gfa_text(text)
+    assert g.seqs() == [b"ACGT", b"NNNNN", b"GG"]
+    assert "without a sequence" in G.last_error()
