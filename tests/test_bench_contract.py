@@ -1,0 +1,48 @@
+"""bench.py pieces that run without a GPU: the reference arm's JSON line (the oracle port on the
+host cores), the clock summary that rejects throttled runs, and the algorithmic-bytes formula of
+the roofline."""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+
+def test_reference_arm_line():
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload", "config1",
+                        "--steps", "1", "--warmup", "3", "--ref-step-seconds", "0.2"],
+                       capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    for k in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in line, k
+    assert line["impl"] == "reference" and line["value"] > 0 and line["warmup"] >= 3
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+
+
+def test_clock_summary_reports_throttle_reasons():
+    import bench
+    c = bench.ClockSampler(0)
+    c.lines = ["0, 1965, 1965, 700.1, 0x0, Not Active, Not Active, Not Active, Not Active",
+               "0, 1900, 1965, 990.0, 0x4, Not Active, Not Active, Not Active, Active",
+               "0, 1950, 1965, 990.0, 0x8, Active, Not Active, Not Active, Not Active",
+               "garbage"]
+    s = c.summary()
+    assert s["sm_mhz"] == 1950 and s["sm_max_mhz"] == 1965 and s["samples"] == 3
+    assert s["reasons"] == ["hw_slowdown", "sw_power_cap"]
+    c.lines = []
+    assert c.summary()["samples"] == 0
+
+
+def test_algorithmic_bytes():
+    import bench
+    lens = np.array([1000, 2000])
+    W = np.array([10, 20])
+    E = np.array([100, 200])
+    assert bench.algorithmic_bytes(lens, W, E) == (1000 + 4 + 320 + 200) + (2000 + 4 + 640 + 400)
