@@ -149,6 +149,7 @@ struct Gfa {
 	std::vector<char> seq_pool;
 	std::vector<Arc> arc;
 	std::vector<uint64_t> idx; // per vertex: first << 32 | n
+	int threads = 1;           // for the parallel steps of finalize (the parse's thread count)
 
 	int64_t find_seg(std::string_view name) const { return names.find(name, NameTable::hash(name)); }
 	uint32_t add_seg(std::string_view name) { return add_seg(name, NameTable::hash(name)); }
@@ -411,30 +412,63 @@ void fix_semi_arc(Gfa &g) // gfa-base.c:269-301
 	}
 }
 
-void fix_symm_add(Gfa &g) // gfa-base.c:303-338
+// For each arc e = v -> w, the first arc of w^1's list that could be its complement (not
+// deleted, w^1 -> v^1 with the overlaps swapped), whether or not an earlier arc claims it; -1 if
+// none. Read-only over the arcs, so it runs on threads for large graphs.
+std::vector<int64_t> complement_candidates(const Gfa &g, size_t n0)
 {
-	uint32_t nvt = g.n_vtx();
-	size_t n0 = g.arc.size();
-	g.arc.reserve(2 * n0); // at most one complement per arc
-	for (uint32_t v = 0; v < nvt; ++v) {
-		uint32_t nv = g.arc_n(v), ofs = g.arc_off(v);
-		for (uint32_t i = 0; i < nv; ++i) {
-			// the index entries of the complement lists a few arcs ahead (random accesses)
-			if (ofs + i + 8 < n0) __builtin_prefetch(g.idx.data() + (g.arc[ofs + i + 8].w ^ 1));
-			Arc avi = g.arc[ofs + i];
-			if (avi.del || avi.comp) continue;
-			uint32_t nw = g.arc_n(avi.w ^ 1), ow_ = g.arc_off(avi.w ^ 1), j;
-			for (j = 0; j < nw; ++j) {
-				Arc &awj = g.arc[ow_ + j];
-				if (awj.del || awj.comp) continue;
-				if (awj.w == (v ^ 1) && awj.ov == avi.ow && awj.ow == avi.ov) {
-					awj.comp = true;
-					awj.link_id = avi.link_id;
+	std::vector<int64_t> cand(n0, -1);
+	auto scan = [&](size_t lo, size_t hi) {
+		for (size_t e = lo; e < hi; ++e) {
+			const Arc &avi = g.arc[e];
+			if (avi.del) continue;
+			const uint32_t v = avi.head(), nw = g.arc_n(avi.w ^ 1), ow_ = g.arc_off(avi.w ^ 1);
+			for (uint32_t j = 0; j < nw; ++j) {
+				const Arc &awj = g.arc[ow_ + j];
+				if (!awj.del && awj.w == (v ^ 1) && awj.ov == avi.ow && awj.ow == avi.ov) {
+					cand[e] = (int64_t)ow_ + j;
 					break;
 				}
 			}
-			if (j == nw) g.add_arc(avi.w ^ 1, v ^ 1, avi.ow, avi.ov, (int64_t)avi.link_id, true);
 		}
+	};
+	const size_t nt = std::max<size_t>(1, (size_t)g.threads);
+	std::vector<std::thread> th;
+	for (size_t t = 1; t < nt; ++t) th.emplace_back(scan, n0 * t / nt, n0 * (t + 1) / nt);
+	scan(0, n0 / nt);
+	for (auto &x : th) x.join();
+	return cand;
+}
+
+void fix_symm_add(Gfa &g) // gfa-base.c:303-338
+{
+	// arcs in order (the lists are sorted by head, so list order is array order); each claims
+	// the first unclaimed complement of its target's list, or gets a new complement arc. The
+	// candidates come precomputed; a claimed candidate sends the arc back to the plain scan.
+	const size_t n0 = g.arc.size();
+	const std::vector<int64_t> cand = complement_candidates(g, n0);
+	g.arc.reserve(2 * n0); // at most one complement per arc
+	for (size_t e = 0; e < n0; ++e) {
+		const Arc avi = g.arc[e];
+		if (avi.del || avi.comp) continue;
+		int64_t j = cand[e];
+		if (j >= 0 && g.arc[(size_t)j].comp) {
+			const uint32_t v = avi.head(), nw = g.arc_n(avi.w ^ 1), ow_ = g.arc_off(avi.w ^ 1);
+			j = -1;
+			for (uint32_t t = 0; t < nw; ++t) {
+				const Arc &awj = g.arc[ow_ + t];
+				if (awj.del || awj.comp) continue;
+				if (awj.w == (v ^ 1) && awj.ov == avi.ow && awj.ow == avi.ov) {
+					j = (int64_t)ow_ + t;
+					break;
+				}
+			}
+		}
+		if (j >= 0) {
+			g.arc[(size_t)j].comp = true;
+			g.arc[(size_t)j].link_id = avi.link_id;
+		} else
+			g.add_arc(avi.w ^ 1, avi.head() ^ 1, avi.ow, avi.ov, (int64_t)avi.link_id, true);
 	}
 	if (g.arc.size() > n0) {
 		g.arc_sort();
@@ -612,6 +646,7 @@ bool read_gfa_parallel(const char *text, size_t len, Gfa &g)
 		const char *nl = (const char *)memchr(p, '\n', (size_t)(text + len - p));
 		cut[(size_t)t] = nl ? nl + 1 : text + len;
 	}
+	g.threads = nt;
 	std::vector<Chunk> ch((size_t)nt);
 	std::vector<std::thread> th;
 	for (int t = 1; t < nt; ++t) th.emplace_back(scan_chunk, cut[(size_t)t], cut[(size_t)t + 1], std::ref(ch[(size_t)t]));
