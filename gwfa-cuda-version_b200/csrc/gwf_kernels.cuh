@@ -71,6 +71,8 @@ struct SrvParams {
 	uint32_t qmask, cmask;
 	int32_t cq_shift;                  // log2(cmask + 1)
 	int32_t dens_milli, flags;
+	int32_t max_lag;                   // > 0: lag pruning of each read (GWF_F_MAX_LAG)
+	int32_t pad_;
 	int64_t idle_ns;                   // the leader warp closes the kernel after this idle
 	                                   // time when no warp is busy
 	int64_t max_idle_ns;               // any warp closes it after this idle time
@@ -999,7 +1001,7 @@ __global__ void __launch_bounds__(256, 3) k_serve(const __grid_constant__ SrvPar
 			lp.r.n = 1;
 			lp.dens_milli = p.dens_milli;
 			lp.flags = p.flags;
-			lp.max_lag = 0;
+			lp.max_lag = p.max_lag;
 			lp.dist = &hdr->dist;
 			lp.status = &hdr->status;
 			align_read(lp, 0, ab + qb, ql, level);

@@ -125,7 +125,7 @@ struct gwf_srv_s {
 	const gwf_graph_t *g = nullptr;
 	GraphDev *G = nullptr;
 	int device = 0, sm_count = 0, ctas = 0;
-	int32_t flags = 0;
+	int32_t flags = 0, max_lag = 0;
 	int64_t budget = 0;
 	uint32_t qcap = 0, ccap = 0;
 	int cq_shift = 0;
@@ -370,6 +370,7 @@ int launch(gwf_srv_s *S)
 	p.cq_shift = S->cq_shift;
 	p.dens_milli = S->G->dens_milli;
 	p.flags = S->flags;
+	p.max_lag = S->max_lag;
 	p.idle_ns = kIdleNs;
 	p.max_idle_ns = kMaxIdleNs;
 	if (gwf_launch_serve(p, S->ctas, 256, S->kstream) != cudaSuccess) return -1;
@@ -464,6 +465,7 @@ extern "C" gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t 
 	gwf_srv_s *S = new gwf_srv_s;
 	S->g = g, S->G = G, S->device = dev;
 	S->flags = opt ? opt->flags : 0;
+	S->max_lag = opt && (opt->flags & GWF_F_MAX_LAG) && opt->max_lag > 0 ? opt->max_lag : 0;
 	size_t fr = 0, tot = 0;
 	cudaMemGetInfo(&fr, &tot);
 	S->budget = opt && opt->arena_budget_bytes > 0 ? opt->arena_budget_bytes : (int64_t)(fr / 4);

@@ -221,7 +221,8 @@ typedef struct {
 	int32_t max_inflight_reads; /* reads admitted at once (queued or running); 0 = 16384 */
 	int32_t flags;              /* GWF_F_* */
 	int32_t device;
-	int32_t reserved[7];
+	int32_t max_lag;            /* with GWF_F_MAX_LAG in flags: the lag of the pruning */
+	int32_t reserved[6];
 } gwf_srv_opts_t;
 gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t *opt);
 /* Queues one request of n reads; returns a request id >= 0 or a GWF_E_* code. Copies the

@@ -61,6 +61,34 @@ def test_mixed_requests_equal_solo_results(G):
     assert stats["launches"] >= 1 and stats["arena_used"] == 0
 
 
+def test_lag_pruning_in_serving_equals_batch(G):
+    """GWF_F_MAX_LAG through the serving options: each read gets the pruned distance that
+    gwf_ed_batch gives with the same lag (and the lag is applied: some reads differ from the
+    exact distance)."""
+    w = G.load_workload("config2", n=300)
+    g = w["graph"]
+    g.index()
+    lag = 2
+    srv = G.Server(g, flags=G.GWF_F_MAX_LAG, max_lag=lag)
+    try:
+        ids = []
+        for r in _requests(w, np.random.default_rng(9)):
+            reads, v0 = _subset(w, r)
+            ids.append((r, srv.submit(reads, v0)))
+        served = [(r, srv.wait(rid, k, timeout_s=300)) for r, (rid, k) in ids]
+    finally:
+        srv.close()
+    d_all = np.empty(300, dtype=np.int32)
+    for r, (d, st) in served:
+        assert (st == 0).all()
+        d_all[r] = d
+    reads = (w["cat"], w["offs"], w["lens"])
+    pruned, _ = g.ed_batch(reads, w["v0"], flags=G.GWF_F_MAX_LAG, max_lag=lag)
+    exact, _ = g.ed_batch(reads, w["v0"])
+    assert np.array_equal(d_all, pruned)
+    assert (pruned != exact).any()
+
+
 def test_small_arena_budget_and_target_vertex(G):
     """An 8 MiB arena budget (a few dozen small arenas at once, one of the largest class): admission
     waits for memory. Requests with a target vertex (v1 >= 0) are mixed with v1 = -1 ones, on a
