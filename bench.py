@@ -313,6 +313,80 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def run_features(args):
+    """The options beyond the reference, each timed end to end (host arrays in, results out) on
+    one GPU: traceback (paths, then paths and CIGARs) against distances alone, opt-in lag
+    pruning against exact distances, and lag pruning in the serving loop. One JSON line."""
+    G = pkg()
+
+    def best_of(fn, k=3):
+        fn()
+        ts = []
+        for _ in range(k):
+            t0 = time.perf_counter()
+            res = fn()
+            ts.append(time.perf_counter() - t0)
+        return min(ts), res
+
+    out = {"metric": "options beyond the reference: traceback, lag pruning, serving with lag pruning",
+           "unit": "reads/s", "n_gpus": 1, "dtype": "int32", "data": "synthetic"}
+    trace = {}
+    for name, n, max_nv, max_ops in (("config2", 100000, 64, 256), ("config4", 2000, 1024, 2048)):
+        w = G.load_workload(name, n=n)
+        g = w["graph"]
+        g.index()
+        reads = (w["cat"], w["offs"], w["lens"])
+        t_d, _ = best_of(lambda: g.ed_batch(reads, w["v0"], mode=G.MODE_PLAIN))
+        t_p, rp = best_of(lambda: g.ed_path(reads, w["v0"], max_nv=max_nv, as_arrays=True))
+        t_c, rc = best_of(lambda: g.ed_path(reads, w["v0"], max_nv=max_nv, as_arrays=True, max_ops=max_ops))
+        trace[name] = {"reads": n, "distance_only": n / t_d, "paths": n / t_p, "paths_and_cigars": n / t_c,
+                       "mean_path_vertices": float(np.mean(rp[3])), "cigars": int((rc[6] > 0).sum())}
+        g.close()
+    out["traceback"] = trace
+    lag = {}
+    for name, n in (("config3", 50000), ("config4", 2000)):
+        w = G.load_workload(name, n=n)
+        g = w["graph"]
+        g.index()
+        reads = (w["cat"], w["offs"], w["lens"])
+        t0, d0 = best_of(lambda: g.ed_batch(reads, w["v0"], mode=G.MODE_PERSISTENT)[0])
+        row = {"reads": n, "exact": n / t0}
+        for m in (5, 20):
+            t, d = best_of(lambda: g.ed_batch(reads, w["v0"], mode=G.MODE_PERSISTENT, flags=G.GWF_F_MAX_LAG,
+                                              max_lag=m)[0])
+            row["lag%d" % m] = {"reads_per_s": n / t, "worse": int(((d != d0) & (d >= 0)).sum()),
+                                "none": int((d < 0).sum())}
+        lag[name] = row
+        g.close()
+    out["lag_pruning"] = lag
+    w = G.load_workload("config5", n=3000)
+    g = w["graph"]
+    g.index()
+    reqs = make_requests(w, np.random.default_rng(55))
+    srv_rows, dists = {}, {}
+    for label, kw in (("exact", {}), ("lag20", {"flags": G.GWF_F_MAX_LAG, "max_lag": 20})):
+        srv = G.Server(g, arena_budget_bytes=int(args.serve_budget_gib * (1 << 30)), **kw)
+        serve_stream(srv, reqs[:3], 0, np.random.default_rng(1))
+        t0 = time.perf_counter()
+        ids = [srv.submit(reads, v0) for reads, v0 in reqs]
+        lat, ds = [], []
+        for rid, k in ids:
+            d, st = srv.wait(rid, k, timeout_s=600)
+            ts, _, td = srv.times(rid)
+            lat.append(td - ts)
+            ds.append(d)
+        span = time.perf_counter() - t0
+        srv.close()
+        srv_rows[label] = {"reads_per_s": len(w["lens"]) / span, "p50_s": float(np.percentile(lat, 50)),
+                           "p99_s": float(np.percentile(lat, 99))}
+        dists[label] = np.concatenate(ds)
+    srv_rows["requests"] = len(reqs)
+    srv_rows["same_distances"] = int((dists["exact"] == dists["lag20"]).sum())
+    srv_rows["reads"] = len(w["lens"])
+    out["serving_all_at_once"] = srv_rows
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -333,6 +407,8 @@ def main():
     ap.add_argument("--reads", type=int, default=0,
                     help="the first N reads of the workload (small profiling cases); 0 = all")
     ap.add_argument("--serving", action="store_true", help="serving benchmark (config5) instead")
+    ap.add_argument("--features", action="store_true",
+                    help="time traceback, lag pruning and serving with lag pruning instead")
     ap.add_argument("--serve-reads", type=int, default=6000)
     ap.add_argument("--serve-budget-gib", type=float, default=64.0)
     ap.add_argument("--plain-sample", type=int, default=6)
@@ -340,6 +416,9 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.serving:
         run_serving(args)
+        return
+    if args.features:
+        run_features(args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
