@@ -46,3 +46,17 @@ def test_algorithmic_bytes():
     W = np.array([10, 20])
     E = np.array([100, 200])
     assert bench.algorithmic_bytes(lens, W, E) == (1000 + 4 + 320 + 200) + (2000 + 4 + 640 + 400)
+
+
+def test_serving_request_split_and_fifo_replay(G):
+    """The serving benchmark's request split covers every read once, in order, in requests of
+    1..256 reads; the plain baseline's FIFO replay queues requests behind each other."""
+    import bench
+    w = G.load_workload("config1", n=1000)
+    reqs = bench.make_requests(w, np.random.default_rng(55))
+    lens = [len(v0) for _, v0 in reqs]
+    assert sum(lens) == 1000 and all(1 <= k <= 256 for k in lens)
+    offs = np.concatenate([reads[1] for reads, _ in reqs])
+    assert np.array_equal(offs, w["offs"])
+    lat = bench.fifo_replay([0.0, 0.0, 5.0], [2.0, 2.0, 1.0])
+    assert list(lat) == [2.0, 4.0, 1.0]
