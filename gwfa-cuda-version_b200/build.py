@@ -50,7 +50,7 @@ def build(force=False, ptxas=False, verbose=False):
     # the gwf-test compatible command-line driver, linked against the library next to it
     cxx = os.environ.get("CXX", "g++")
     cmd = [cxx, "-O2", "-std=c++17", "-o", CLI, os.path.join(CSRC, "gwf_cli.cpp"), "-L" + HERE, "-lgwfa_b200",
-           "-Wl,-rpath,$ORIGIN", "-lz"]
+           "-Wl,-rpath,$ORIGIN", "-lpthread"]
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, capture_output=True, text=True)

@@ -22,6 +22,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/gwfa.h"
@@ -75,9 +76,20 @@ int main(int argc, char *argv[])
 		usage();
 		return 1;
 	}
+	// the reads load on a second thread while the graph loads (the error text is per thread)
+	gwf_reads_t *rs = nullptr;
+	std::string reads_err;
+	std::thread reader;
+	if (!print_graph)
+		reader = std::thread([&] {
+			rs = gwf_reads_load(argv[i + 1]);
+			if (!rs) reads_err = gwf_last_error();
+		});
 	gwf_graph_t *g = gwf_gfa_load(argv[i], sname);
+	if (reader.joinable()) reader.join();
 	if (!g) {
 		fprintf(stderr, "ERROR: %s\n", gwf_last_error());
+		gwf_reads_free(rs);
 		return 1;
 	}
 	if (print_graph) {
@@ -89,9 +101,8 @@ int main(int argc, char *argv[])
 		return 0;
 	}
 	// the reads, concatenated, through the library's reader (FASTA/FASTQ, plain or gzip)
-	gwf_reads_t *rs = gwf_reads_load(argv[i + 1]);
 	if (!rs) {
-		fprintf(stderr, "ERROR: cannot read %s: %s\n", argv[i + 1], gwf_last_error());
+		fprintf(stderr, "ERROR: cannot read %s: %s\n", argv[i + 1], reads_err.c_str());
 		gwf_graph_free(g);
 		return 1;
 	}
