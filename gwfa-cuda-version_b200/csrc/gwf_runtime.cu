@@ -903,6 +903,9 @@ static int launch_cigar(Engine &E, const GraphDev &G, Batch &B, TraceBufs &T, co
 		CK(cudaStreamSynchronize(E.stream)); // arenas and offsets are reused by the next chunk
 		start = end;
 	}
+	// the memset above is on a non-blocking stream: done before the caller copies cigar_n back,
+	// also when no read was launched
+	CK(cudaStreamSynchronize(E.stream));
 	return 0;
 }
 
