@@ -66,6 +66,8 @@ static int noalloc_setup(int dev, cudaStream_t stream, uint8_t **out)
 		}
 		k_noalloc_init<<<64, 256, 0, stream>>>((uint8_t *)ptr);
 		e = cudaGetLastError();
+		// the tables must be written before any call, from any thread or stream, reads them
+		if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
 		if (e != cudaSuccess) {
 			gwf_set_errorf("gwf_ed_batch_noalloc: set-up kernel failed: %s", cudaGetErrorString(e));
 			return GWF_E_CUDA;
@@ -88,6 +90,10 @@ extern "C" int gwf_ed_batch_noalloc(const gwf_graph_t *g, int32_t n, int32_t max
 	if (max_ql > kMaxQl) {
 		gwf_set_errorf("gwf_ed_batch_noalloc: reads of %d bases exceed the fixed limit of %d", max_ql, kMaxQl);
 		return GWF_E_CAPACITY;
+	}
+	if (flags & ~GWF_F_EXACT_START) {
+		gwf_set_error("gwf_ed_batch_noalloc: only GWF_F_EXACT_START is honoured (no lag pruning here)");
+		return GWF_E_BAD_INPUT;
 	}
 	if (n == 0) return 0;
 	if (!g || !d_seqs || !d_offs || !d_ql || !d_v0 || !d_dist || !d_status || max_ql <= 0) {
@@ -120,11 +126,14 @@ extern "C" int gwf_ed_batch_noalloc(const gwf_graph_t *g, int32_t n, int32_t max
 
 	const Caps c = caps_for(kMaxQl, 0, G->dens_milli);
 	const int64_t slot = ws_layout(c).total;
+	// warps that the scratch holds, at most two CTAs per SM, and no more CTAs than the reads need;
+	// a CTA's warps that find the queue empty leave at once
 	int64_t warps = (kScratchBytes - kOffArena) / slot;
 	int sms = 0;
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	warps = warps < (int64_t)sms * 2 * kWarpsPerCta ? warps : (int64_t)sms * 2 * kWarpsPerCta;
-	warps = warps < n ? warps : n;
+	const int64_t need = ((int64_t)n + kWarpsPerCta - 1) / kWarpsPerCta * kWarpsPerCta;
+	warps = warps < need ? warps : need;
 	warps = (warps / kWarpsPerCta) * kWarpsPerCta;
 	if (warps < kWarpsPerCta) {
 		gwf_set_errorf("gwf_ed_batch_noalloc: one warp arena (%lld bytes for this graph) does not fit the "

@@ -176,11 +176,13 @@ void gwf_batch_destroy(gwf_batch_t *b);
  * outgrows its arena gets per-read status GWF_E_CAPACITY (there is no larger arena to retry in).
  * Layout: read i is d_seqs[d_offs[i] .. d_offs[i]+d_ql[i]); d_seqs must be 8-byte aligned with
  * 16 readable bytes after the last read. The graph must have been indexed on the current device
- * (gwf_ed_index). Asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream):
- * d_dist / d_status are valid once the stream has completed. The first call on a device does a
- * one-time set-up (symbol lookup and a small init kernel); make that first call before any
- * stream capture. All calls share the one array, so calls that overlap on the GPU (e.g. on two
- * streams) race; serialise them. Returns 0 or a GWF_E_* code. */
+ * (gwf_ed_index). flags: only GWF_F_EXACT_START is honoured; any other bit returns
+ * GWF_E_BAD_INPUT (this call has no lag pruning). Asynchronous on `stream` (a cudaStream_t, NULL =
+ * legacy default stream): d_dist / d_status are valid once the stream has completed. The first
+ * call on a device does a one-time set-up (symbol lookup, a small init kernel, and a wait for it
+ * on `stream`); make that first call before any stream capture. All calls share the one array,
+ * so calls that overlap on the GPU (e.g. on two streams) race; serialise them. Returns 0 or a
+ * GWF_E_* code. */
 #define GWF_NOALLOC_MAX_READS     262144
 #define GWF_NOALLOC_MAX_QL        2048
 #define GWF_NOALLOC_SCRATCH_BYTES (64LL << 20)

@@ -29,7 +29,7 @@ ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
 GOLD = os.path.join(ROOT, "tests", "golden")
 INP = os.path.join(ROOT, "_work", "golden_inputs")
 OUT = None  # the reference outputs' directory, from the command line
-REF = "/root/reference"
+REF = os.environ.get("GWF_REFERENCE_DIR", "/root/reference")  # the reference source tree
 
 # synthetic sets: name -> (workload, n reads)
 SYNTH = {"config1": ("config1", 1000), "config2": ("config2", 2000), "config3": ("config3", 600),
@@ -74,7 +74,7 @@ def write_fasta(path, reads):
 def prepare():
     G, O = pkg(), oracle()
     os.makedirs(INP, exist_ok=True)
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all", "ref"], check=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all", "ref", "REF=" + REF], check=True)
     gwf_test = os.path.join(ROOT, "oracle", "_ref", "gwf-test")
     shutil.copy(os.path.join(REF, "exposed_testing/1000_reads/graph_1000.gfa"), GOLD)
     shutil.copy(os.path.join(REF, "exposed_testing/generated/grafo_test.gfa"), GOLD)
