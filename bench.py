@@ -1,15 +1,17 @@
 """Benchmark of the GWFA sequence-to-graph edit-distance path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload config2] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload config3] [--impl ours|reference]
 
-One step = one pass of the path over the whole workload (default: 100,000 reads of 1 kbp, 50,000
-at 5% and 50,000 at 10% error, on the 100 kbp bubble graph; synthetic and seeded). `value` is
-reads/s with the reads already resident in HBM (CUDA events on the library's stream, L2 flushed
-between steps); `e2e` is the same metric through gwf_ed_batch_concat from pinned host memory,
-with the copies in the timed region. Under torchrun every rank aligns its own workload (weak
-scaling, no data-path collective); timings are the max over ranks.
+One step = one pass of the path over the whole workload (default: the mixed-length batch, 200,000
+reads with lognormal lengths of median 2 kbp in [500, 10000] bp and error rates U[1%, 10%], on the
+100 kbp bubble graph; synthetic and seeded), in the persistent form, beside the plain form on the
+same reads. `value` is reads/s with the reads already resident in HBM (CUDA events on the
+library's stream, L2 flushed between steps); `e2e` is the same metric through gwf_ed_batch_concat
+from pinned host memory, with the copies in the timed region. Under torchrun every rank aligns
+its own workload (weak scaling, no data-path collective); timings are the max over ranks.
 `--impl reference` times the reference algorithm on the host cores instead (the reference ships
-no CPU gwf_ed; its CPU restatement in oracle/ stands in for it).
+no CPU gwf_ed; its CPU restatement in oracle/ stands in for it, on inputs made by the same seeded
+generator compiled into oracle/liboracle.so, so that arm maps no library of the product).
 """
 import argparse
 import ctypes
@@ -162,14 +164,29 @@ def cpu_oracle_run(w, max_seconds=30.0, threads=0):
             "threads": used, "full": len(sel) == n}
 
 
+def mapped_libraries():
+    """Shared objects of this repository mapped into the process (from /proc/self/maps)."""
+    out = set()
+    try:
+        for line in open("/proc/self/maps"):
+            f = line.split()
+            if len(f) >= 6 and f[-1].endswith(".so") and f[-1].startswith(ROOT):
+                out.add(os.path.relpath(f[-1], ROOT))
+    except OSError:
+        pass
+    return sorted(out)
+
+
 def run_reference(args, rank, world):
-    """Reference arm: the reference algorithm on the host cores (oracle port, all threads)."""
+    """Reference arm: the reference algorithm on the host cores (oracle port, all threads). The
+    workload comes from the same seeded generator compiled into liboracle.so, so this process
+    maps no library of the product."""
     if rank != 0:
         return
-    G = pkg()
-    w = G.load_workload(args.workload)
+    spec = pkg().workload_spec(args.workload)  # plain data: the package's library is not loaded
     O = oracle_mod()
-    og = O.OracleGraph.from_graph(w["graph"])
+    w = O.synth_workload(spec)
+    og = w["graph"]
     n = len(w["lens"])
     # each step aligns a bounded, evenly spread sample so the whole run takes a few minutes
     budget_s = args.ref_step_seconds
@@ -192,11 +209,14 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": rps, "unit": "reads/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC[args.workload], "sample_reads_per_step": m},
+        "config": {"workload": WORKLOAD_DESC[args.workload], "reads_per_gpu": n,
+                   "l2": "not applicable: host cores",
+                   "parallelism": "all host threads, one process (an evenly spread sample per step)"},
         "gbases_per_s": bases / (ms / 1000.0) / 1e9,
         "cpu_baseline": {"value": rps, "unit": "reads/s", "cores": threads, "kind": "port",
                          "sample": "%d of %d reads per step, evenly spread" % (m, n)},
         "e2e": {"value": rps, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "libraries_mapped": mapped_libraries(),
     }
     print(json.dumps(line), flush=True)
 
@@ -392,12 +412,12 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="config2", choices=sorted(WORKLOAD_DESC))
+    ap.add_argument("--workload", default="config3", choices=sorted(WORKLOAD_DESC))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="persistent", choices=["persistent", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--ref-step-seconds", type=float, default=8.0)
+    ap.add_argument("--ref-step-seconds", type=float, default=6.0)
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="persistent grid; 0 = occupancy limit")
     ap.add_argument("--graph", type=int, default=1, help="1 = persistent runs replay a captured CUDA graph")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
@@ -498,6 +518,7 @@ def main():
         forms = {args.mode: n / (ms / 1000.0),
                  ("plain" if other == G.MODE_PLAIN else "persistent"): n / (ms2 / 1000.0),
                  "forms_identical": bool(np.array_equal(d2, dist_gpu))}
+        forms["persistent_over_plain"] = forms["persistent"] / forms["plain"]
 
     # end to end through the public batch call, pinned host buffers, copies in the timed region
     e2e_t = []
@@ -526,11 +547,11 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "strong" if args.split else "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC[args.workload], "reads_per_gpu": n, "form": args.mode,
-                   "cuda_graph": bool(use_graph),
+        "config": {"workload": WORKLOAD_DESC[args.workload], "reads_per_gpu": n,
                    "l2": "flushed between steps (256 MB write)",
                    "parallelism": ("one batch split by cost over the ranks, distances all-gathered, graph replicated"
                                    if args.split else "reads sharded by rank, graph replicated")},
+        "form": args.mode, "cuda_graph": bool(use_graph),
         "gbases_per_s": job_bases / (ms / 1000.0) / 1e9,
         "e2e": ({"value": job_reads / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
                 if e2e_s else None),

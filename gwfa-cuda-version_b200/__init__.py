@@ -612,8 +612,10 @@ class SynthGraph:
             pass
 
 
-def load_workload(kind, n=None, seed=None, pinned=False):
-    """Synthetic workloads of the five benchmark configurations (seeded).
+def workload_spec(kind, n=None, seed=None):
+    """Parameters of the five seeded benchmark workloads, as plain data (no library call):
+    {"graph": gwf_synth_graph_new arguments, "parts": [gwf_synth_reads_new arguments after the
+    graph, one tuple per read set]}.
 
     config1: 100 kbp graph, 1,000 x 1 kbp reads at 1%
     config2: same graph, 100,000 x 1 kbp reads (50,000 at 5%, 50,000 at 10%)
@@ -621,49 +623,63 @@ def load_workload(kind, n=None, seed=None, pinned=False):
              [500, 10000], error U[1%, 10%]
     config4: 5 Mbp graph (site every 50 bp, SV every 50 kbp), 20,000 x 10 kbp reads at 5%
     config5: config-4 graph, reads of U[500, 20000] bp at U[1%, 10%] (serving requests)
-    Returns dict(graph=Graph, synth=SynthGraph, cat, offs, lens, v0, err).
     """
     if kind in ("config1", "config2", "config3"):
-        sg = SynthGraph(100_000, 500, 0.7, 10, 0, 0, 0, seed=1)
+        graph = (100_000, 500, 0.7, 10, 0, 0, 0, 1)
     elif kind in ("config4", "config5"):
-        sg = SynthGraph(5_000_000, 50, 0.7, 20, 50_000, 1000, 5000, seed=4)
+        graph = (5_000_000, 50, 0.7, 20, 50_000, 1000, 5000, 4)
     else:
         raise ValueError(kind)
-    g = Graph.from_gfa_text(sg.gfa)
-    seg2v = g.vertex_of_segment()
-    parts = []
     if kind == "config1":
-        parts.append(sg.reads(n or 1000, 0, 1000, 0, 1000, 1000, 0.01, 0.01, seed if seed is not None else 11, pinned))
+        parts = [(n or 1000, 0, 1000, 0, 1000, 1000, 0.01, 0.01, seed if seed is not None else 11)]
     elif kind == "config2":
         h = (n or 100_000) // 2
-        parts.append(sg.reads(h, 0, 1000, 0, 1000, 1000, 0.05, 0.05, 21 if seed is None else seed, pinned))
-        parts.append(sg.reads((n or 100_000) - h, 0, 1000, 0, 1000, 1000, 0.10, 0.10, 22 if seed is None else seed + 1, pinned))
+        parts = [(h, 0, 1000, 0, 1000, 1000, 0.05, 0.05, 21 if seed is None else seed),
+                 ((n or 100_000) - h, 0, 1000, 0, 1000, 1000, 0.10, 0.10, 22 if seed is None else seed + 1)]
     elif kind == "config3":
-        parts.append(sg.reads(n or 200_000, 1, 2000, 0.6, 500, 10000, 0.01, 0.10, 3 if seed is None else seed, pinned))
+        parts = [(n or 200_000, 1, 2000, 0.6, 500, 10000, 0.01, 0.10, 3 if seed is None else seed)]
     elif kind == "config4":
-        parts.append(sg.reads(n or 20_000, 0, 10000, 0, 10000, 10000, 0.05, 0.05, 41 if seed is None else seed, pinned))
+        parts = [(n or 20_000, 0, 10000, 0, 10000, 10000, 0.05, 0.05, 41 if seed is None else seed)]
     else:
-        parts.append(sg.reads(n or 1000, 2, 500, 20000, 500, 20000, 0.01, 0.10, 5 if seed is None else seed, pinned))
+        parts = [(n or 1000, 2, 500, 20000, 500, 20000, 0.01, 0.10, 5 if seed is None else seed)]
+    return {"graph": graph, "parts": parts}
+
+
+def concat_parts(parts, alloc=None):
+    """Read sets (dicts of cat, offs, lens, origin_seg, err) -> one concatenated set; alloc(nbytes)
+    returns the uint8 array that receives the bytes (pinned memory), default numpy."""
     if len(parts) == 1:
         p = parts[0]
-        cat, offs, lens, org, err = p["cat"], p["offs"], p["lens"], p["origin_seg"], p["err"]
-    else:
-        base = 0
-        cats, offss = [], []
-        for p in parts:
-            tot = int(p["offs"][-1] + p["lens"][-1]) if len(p["lens"]) else 0
-            cats.append(p["cat"][:tot])
-            offss.append(p["offs"] + base)
-            base += tot
-        cat = np.concatenate(cats + [np.zeros(16, np.uint8)])
-        if pinned:
-            raw = lib().gwf_pinned_alloc(len(cat))
-            pc = np.ctypeslib.as_array((ctypes.c_uint8 * len(cat)).from_address(raw))
-            pc[:] = cat
-            cat = pc
-        offs = np.concatenate(offss)
-        lens = np.concatenate([p["lens"] for p in parts])
-        org = np.concatenate([p["origin_seg"] for p in parts])
-        err = np.concatenate([p["err"] for p in parts])
+        return p["cat"], p["offs"], p["lens"], p["origin_seg"], p["err"]
+    base = 0
+    cats, offss = [], []
+    for p in parts:
+        tot = int(p["offs"][-1] + p["lens"][-1]) if len(p["lens"]) else 0
+        cats.append(p["cat"][:tot])
+        offss.append(p["offs"] + base)
+        base += tot
+    cat = np.concatenate(cats + [np.zeros(16, np.uint8)])
+    if alloc is not None:
+        pc = alloc(len(cat))
+        pc[:] = cat
+        cat = pc
+    return (cat, np.concatenate(offss), np.concatenate([p["lens"] for p in parts]),
+            np.concatenate([p["origin_seg"] for p in parts]), np.concatenate([p["err"] for p in parts]))
+
+
+def _pinned_array(nbytes):
+    raw = lib().gwf_pinned_alloc(nbytes)
+    return np.ctypeslib.as_array((ctypes.c_uint8 * nbytes).from_address(raw))
+
+
+def load_workload(kind, n=None, seed=None, pinned=False):
+    """Synthetic workloads of the five benchmark configurations (seeded; workload_spec).
+    Returns dict(graph=Graph, synth=SynthGraph, cat, offs, lens, v0, err)."""
+    spec = workload_spec(kind, n, seed)
+    sg = SynthGraph(*spec["graph"][:7], seed=spec["graph"][7])
+    g = Graph.from_gfa_text(sg.gfa)
+    seg2v = g.vertex_of_segment()
+    parts = [sg.reads(*pa[:8], seed=pa[8], pinned=pinned) for pa in spec["parts"]]
+    cat, offs, lens, org, err = concat_parts(parts, _pinned_array if pinned else None)
     v0 = np.array([seg2v[int(o)] for o in org], dtype=np.int32)
     return {"graph": g, "synth": sg, "cat": cat, "offs": offs, "lens": lens, "v0": v0, "err": err}

@@ -130,6 +130,78 @@ class OracleGraph:
             pass
 
 
+def _synth_sigs(L):
+    P, I32, I64, U64, DBL = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double
+    for name, res, args in (("gwf_synth_graph_new", P, [I64, I32, DBL, I32, I32, I32, I32, U64]),
+                            ("gwf_synth_graph_free", None, [P]),
+                            ("gwf_synth_graph_gfa", I64, [P, ctypes.c_char_p, I64]),
+                            ("gwf_synth_reads_new", P, [P, I32, I32, DBL, DBL, I32, I32, DBL, DBL, U64]),
+                            ("gwf_synth_reads_bytes", I64, [P]),
+                            ("gwf_synth_reads_copy", None, [P, P, P, P, P, P]),
+                            ("gwf_synth_reads_free", None, [P])):
+        f = getattr(L, name)
+        f.restype, f.argtypes = res, args
+
+
+def parse_gfa(text):
+    """Segments and links of a GFA text whose links all join forward strands ("L a + b + nM" or
+    "*"), as the seeded generator writes: (seqs in S-line order, arcs (v, w, overlap on w)).
+    Vertex i is the i-th S line."""
+    seqs, name2v, links = [], {}, []
+    for line in text.split(b"\n"):
+        f = line.rstrip(b"\r").split(b"\t")
+        if f[0] == b"S":
+            name2v[f[1]] = len(seqs)
+            seqs.append(f[2])
+        elif f[0] == b"L":
+            if f[2] != b"+" or f[4] != b"+":
+                raise ValueError("parse_gfa: reverse-strand link")
+            ov = f[5] if len(f) > 5 else b"*"
+            links.append((f[1], f[3], 0 if ov in (b"*", b"") else int(ov.rstrip(b"M"))))
+    return seqs, [(name2v[a], name2v[b], o) for a, b, o in links]
+
+
+def synth_workload(spec):
+    """The seeded workload of a spec (the product package's workload_spec: graph arguments and
+    read sets), made with the generator compiled into liboracle.so, as an OracleGraph plus the
+    concatenated reads. Loads no product library: the CPU baseline's own input path. Vertices
+    are numbered in S-line order; the distances equal those on the product's loader numbering."""
+    L = lib()
+    _synth_sigs(L)
+    ga = spec["graph"]
+    sg = L.gwf_synth_graph_new(*ga)
+    try:
+        n = L.gwf_synth_graph_gfa(sg, None, 0)
+        buf = ctypes.create_string_buffer(n)
+        L.gwf_synth_graph_gfa(sg, buf, n)
+        seqs, arcs = parse_gfa(buf.raw[:n])
+        parts = []
+        for pa in spec["parts"]:
+            r = L.gwf_synth_reads_new(sg, *pa)
+            tot = L.gwf_synth_reads_bytes(r)
+            m = pa[0]
+            cat = np.zeros(tot + 16, dtype=np.uint8)
+            offs, lens = np.zeros(m, dtype=np.int64), np.zeros(m, dtype=np.int32)
+            org, err = np.zeros(m, dtype=np.int32), np.zeros(m, dtype=np.float32)
+            L.gwf_synth_reads_copy(r, cat.ctypes.data, offs.ctypes.data, lens.ctypes.data, org.ctypes.data,
+                                   err.ctypes.data)
+            L.gwf_synth_reads_free(r)
+            parts.append((cat[:tot], offs, lens, org))
+    finally:
+        L.gwf_synth_graph_free(sg)
+    base, cats = 0, []
+    offs_all, lens_all, org_all = [], [], []
+    for cat, offs, lens, org in parts:
+        cats.append(cat)
+        offs_all.append(offs + base)
+        base += len(cat)
+        lens_all.append(lens)
+        org_all.append(org)
+    cat = np.concatenate(cats + [np.zeros(16, np.uint8)])
+    return {"graph": OracleGraph(seqs, arcs), "cat": cat, "offs": np.concatenate(offs_all),
+            "lens": np.concatenate(lens_all), "v0": np.concatenate(org_all).astype(np.int32)}
+
+
 def stats_arrays(st, n):
     """Stats array -> dict of numpy arrays."""
     out = {}

@@ -24,6 +24,24 @@ def test_reference_arm_line():
     assert line["impl"] == "reference" and line["value"] > 0 and line["warmup"] >= 3
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+    # the arm maps the oracle's library only, never the product's
+    assert line["libraries_mapped"] == ["oracle/liboracle.so"], line["libraries_mapped"]
+
+
+def test_reference_arm_workload_equals_product_workload(G, O):
+    """The reference arm makes its inputs with the generator compiled into liboracle.so and a
+    GFA parse of its own: the same reads, and the same distances as on the product loader's
+    graph (whose vertex numbering differs)."""
+    for kind, n in (("config1", 200), ("config2", 100), ("config3", 100)):
+        w = G.load_workload(kind, n=n)
+        wo = O.synth_workload(G.workload_spec(kind, n))
+        end = int(w["offs"][-1] + w["lens"][-1])
+        assert np.array_equal(w["offs"], wo["offs"]) and np.array_equal(w["lens"], wo["lens"])
+        assert np.array_equal(w["cat"][:end], wo["cat"][:end])
+        d1, _, _ = O.OracleGraph.from_graph(w["graph"]).ed_batch(w["cat"], w["offs"], w["lens"], w["v0"],
+                                                                  stats=False)
+        d2, _, _ = wo["graph"].ed_batch(wo["cat"], wo["offs"], wo["lens"], wo["v0"], stats=False)
+        assert np.array_equal(d1, d2)
 
 
 def test_clock_summary_reports_throttle_reasons():
