@@ -40,6 +40,8 @@ struct DevGraph {
 	const uint8_t *raw;      // raw bytes (buffer 8-byte aligned, +16 padding bytes)
 	const uint32_t *arc_off; // [n_vtx + 1] CSR offsets
 	const uint2 *arc;        // (target, overlap)
+	const uint32_t *arc_key; // vertex part of the arrival key per arc (entry id), or null when
+	                         // every vertex's in-arcs share one overlap (the key is the target)
 	uint32_t n_vtx;
 	int32_t pure;            // 1 when every graph byte is A/C/G/T
 };

@@ -395,7 +395,10 @@ __device__ __noinline__ void align_read_t(const KParams &p, int32_t r, uint8_t *
 						const uint2 e = __ldg(g.arc + aoff + t);
 						w = e.x, ol = (int32_t)e.y;
 						if (isv) {
-							const int ins = hset_insert(h, hmask, (uint64_t)w << 32 | (uint32_t)(i + 1));
+							// arrival key (w, i + 1) as in the reference (gwf-ed.cu:1196), or the
+							// arc's entry id in place of w where w's in-arcs differ in overlap
+							const uint32_t kv = g.arc_key ? __ldg(g.arc_key + aoff + t) : w;
+							const int ins = hset_insert(h, hmask, (uint64_t)kv << 32 | (uint32_t)(i + 1));
 							if (ins < 0) ovf = true;
 							const bool absent = ins == 1;
 							if (base_eq(g, rc, w, ol, i + 1)) {

@@ -131,6 +131,7 @@ DevGraph GraphDev::view() const
 	v.raw = (const uint8_t *)raw.p;
 	v.arc_off = (const uint32_t *)arc_off.p;
 	v.arc = (const uint2 *)arc.p;
+	v.arc_key = (const uint32_t *)arc_key.p;
 	v.n_vtx = n_vtx;
 	v.pure = pure;
 	return v;
@@ -142,6 +143,7 @@ GraphDev::~GraphDev()
 	cudaGetDevice(&cur);
 	if (device >= 0) cudaSetDevice(device);
 	len.release(), base.release(), pk.release(), raw.release(), arc_off.release(), arc.release();
+	arc_key.release();
 	if (cur >= 0) cudaSetDevice(cur);
 }
 
@@ -180,6 +182,38 @@ static int upload_graph(const gwf_graph_t *g, GraphDev *G)
 	for (uint32_t v = 0; v < nv; ++v) off[v + 1] += off[v];
 	std::vector<uint2> arc(g->n_arc ? g->n_arc : 1);
 	for (uint32_t e = 0; e < g->n_arc; ++e) arc[e] = make_uint2((uint32_t)g->arc[e].a, (uint32_t)g->arc[e].o);
+	// Arrival keys. The reference keys an arrival by (target w, query position) (gwf-ed.cu:1196),
+	// which names one graph position when every arc into w enters it at the same offset. Where the
+	// arcs into w carry different overlaps, the arcs entering w at one offset share an entry id of
+	// their own (>= n_vtx), so that arrivals at different offsets of w stay distinct.
+	std::vector<int32_t> first(nv, -1);
+	std::vector<uint8_t> mixed(nv, 0);
+	bool any_mixed = false;
+	for (uint32_t e = 0; e < g->n_arc; ++e) {
+		const uint32_t w = (uint32_t)g->arc[e].a;
+		if (first[w] < 0) first[w] = g->arc[e].o;
+		else if (first[w] != g->arc[e].o) mixed[w] = 1, any_mixed = true;
+	}
+	std::vector<uint32_t> key;
+	if (any_mixed) {
+		if ((uint64_t)nv + g->n_arc >= 0xffffffffULL) {
+			gwf_set_error("gwf_ed_index: too many vertices and arcs for the arrival keys");
+			return GWF_E_BAD_GRAPH;
+		}
+		std::vector<std::pair<uint64_t, uint32_t>> t;
+		key.resize(g->n_arc);
+		for (uint32_t e = 0; e < g->n_arc; ++e) {
+			const uint32_t w = (uint32_t)g->arc[e].a;
+			key[e] = w;
+			if (mixed[w]) t.push_back({(uint64_t)w << 32 | (uint32_t)g->arc[e].o, e});
+		}
+		std::sort(t.begin(), t.end());
+		uint32_t next = nv;
+		for (size_t i = 0; i < t.size(); ++i) {
+			if (i > 0 && t[i].first != t[i - 1].first) ++next;
+			key[t[i].second] = next;
+		}
+	}
 	G->n_vtx = nv, G->n_arc = g->n_arc, G->pure = pure, G->total_len = tot;
 	G->dens_milli = (int32_t)std::max<uint64_t>(1, (uint64_t)nv * 1000 / std::max<uint64_t>(1, tot));
 	int rc;
@@ -195,6 +229,10 @@ static int upload_graph(const gwf_graph_t *g, GraphDev *G)
 	CK(cudaMemcpy(G->raw.p, raw.data(), raw.size(), cudaMemcpyHostToDevice));
 	CK(cudaMemcpy(G->arc_off.p, off.data(), sizeof(uint32_t) * (nv + 1), cudaMemcpyHostToDevice));
 	CK(cudaMemcpy(G->arc.p, arc.data(), sizeof(uint2) * arc.size(), cudaMemcpyHostToDevice));
+	if (any_mixed) {
+		if ((rc = G->arc_key.ensure(sizeof(uint32_t) * key.size()))) return rc;
+		CK(cudaMemcpy(G->arc_key.p, key.data(), sizeof(uint32_t) * key.size(), cudaMemcpyHostToDevice));
+	}
 	return 0;
 }
 

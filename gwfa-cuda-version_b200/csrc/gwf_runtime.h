@@ -28,6 +28,7 @@ struct GraphDev { // device-resident copy of one gwf_graph_t
 	int32_t pure = 0, dens_milli = 1;
 	uint64_t total_len = 0;
 	DBuf len, base, pk, raw, arc_off, arc;
+	DBuf arc_key; // entry id per arc, only when some vertex's in-arcs carry different overlaps
 	gwfb::DevGraph view() const;
 	~GraphDev();
 };

@@ -507,7 +507,11 @@ static int o_extend(ows_t *w, int32_t *end_v, int32_t *end_off)
 			for (j = 0; j < nv; ++j) {
 				uint32_t wv = (uint32_t)g->arc[ov + j].a;
 				int32_t ol = g->arc[ov + j].o;
-				int absent = hset_put(w, (uint64_t)wv << 32 | (uint32_t)(ii + 1));
+				/* GWFO_O_ENTRY_KEY: the library's arrival key, whose vertex part is the arc's entry
+				 * id (gwfo_index), so that arrivals at one query position through arcs of different
+				 * overlaps into one vertex stay distinct */
+				uint32_t kv = (w->opts & GWFO_O_ENTRY_KEY) ? (uint32_t)g->aux[g->n_vtx + ov + j] : wv;
+				int absent = hset_put(w, (uint64_t)kv << 32 | (uint32_t)(ii + 1));
 				if (q[ii + 1] == g->seq[wv][ol]) {
 					++n_ext;
 					if (absent) A_push(w, gen_vd(wv, ii + 1 - ol), ol, (x0 + 2) << 1 | 1);
@@ -602,17 +606,54 @@ static int arc_cmp(const void *x, const void *y)
 	return a->a < b->a ? -1 : a->a > b->a ? 1 : 0;
 }
 
+/* entry ids of the arcs, for GWFO_O_ENTRY_KEY (the library's rule, gwf_runtime.cu upload_graph):
+ * the target vertex w when every arc into w has the same overlap, else an id >= n_vtx that is
+ * the same for the arcs into w with the same overlap and differs otherwise */
+typedef struct { uint64_t key; uint32_t e; } oentry_t;
+static int entry_cmp(const void *x, const void *y)
+{
+	const oentry_t *a = (const oentry_t *)x, *b = (const oentry_t *)y;
+	return a->key < b->key ? -1 : a->key > b->key ? 1 : (a->e > b->e) - (a->e < b->e);
+}
+
+static void entry_ids(gwf_graph_t *g, uint64_t *eid)
+{
+	int32_t *first = (int32_t *)malloc(sizeof(int32_t) * (g->n_vtx ? g->n_vtx : 1));
+	uint8_t *mixed = (uint8_t *)calloc(g->n_vtx ? g->n_vtx : 1, 1);
+	oentry_t *t = (oentry_t *)malloc(sizeof(oentry_t) * (g->n_arc ? g->n_arc : 1));
+	uint32_t e, n = 0, v, next = g->n_vtx;
+	for (v = 0; v < g->n_vtx; ++v) first[v] = -1;
+	for (e = 0; e < g->n_arc; ++e) {
+		uint32_t w = (uint32_t)g->arc[e].a;
+		if (first[w] < 0) first[w] = g->arc[e].o;
+		else if (first[w] != g->arc[e].o) mixed[w] = 1;
+	}
+	for (e = 0; e < g->n_arc; ++e) {
+		uint32_t w = (uint32_t)g->arc[e].a;
+		eid[e] = w;
+		if (mixed[w]) t[n].key = (uint64_t)w << 32 | (uint32_t)g->arc[e].o, t[n++].e = e;
+	}
+	qsort(t, n, sizeof(oentry_t), entry_cmp);
+	for (e = 0; e < n; ++e) {
+		if (e > 0 && t[e].key != t[e - 1].key) ++next;
+		eid[t[e].e] = next;
+	}
+	free(first), free(mixed), free(t);
+}
+
 void gwfo_index(gwf_graph_t *g)
 {
 	uint32_t i, st;
 	qsort(g->arc, g->n_arc, sizeof(gwf_arc_t), arc_cmp);
-	g->aux = (uint64_t *)calloc(g->n_vtx ? g->n_vtx : 1, sizeof(uint64_t));
+	/* aux[0 .. n_vtx) is the reference's CSR; aux[n_vtx + e] holds arc e's entry id */
+	g->aux = (uint64_t *)calloc((size_t)g->n_vtx + g->n_arc + 1, sizeof(uint64_t));
 	for (st = 0, i = 1; i <= g->n_arc; ++i)
 		if (i == g->n_arc || g->arc[i].a >> 32 != g->arc[st].a >> 32) {
 			uint32_t v = (uint32_t)(g->arc[st].a >> 32);
 			if (v < g->n_vtx) g->aux[v] = (uint64_t)st << 32 | (i - st);
 			st = i;
 		}
+	entry_ids(g, g->aux + g->n_vtx);
 }
 
 void gwfo_index_free(gwf_graph_t *g)

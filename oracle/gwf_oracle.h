@@ -31,6 +31,12 @@ extern "C" {
 /* options */
 #define GWFO_O_EXACT_START  0x1 /* disable the two k=-1 unsigned-compare rules of the start
                                      state (see gwf_oracle.c): exact edit distance */
+#define GWFO_O_ENTRY_KEY    0x2 /* the library's arrival key: (entry id, query position), the
+                                     entry id telling apart arcs into one vertex with different
+                                     overlaps. The reference keys on (vertex, query position)
+                                     (gwf-ed.cu:1196), so where the arcs into a vertex carry
+                                     different overlaps its result depends on its FIFO order; with
+                                     one overlap per vertex both keys are the same. */
 
 typedef struct {
 	int32_t steps;        /* score steps executed (s + 1 when an end is found) */

@@ -18,6 +18,7 @@ F_SWAP_DROP = 0x002
 F_UNSAFE_MASK = 0x7F0
 F_NONTERM = 0x400
 O_EXACT_START = 0x1
+O_ENTRY_KEY = 0x2
 
 
 class Stats(ctypes.Structure):
@@ -98,15 +99,17 @@ class OracleGraph:
     def arcs_sorted(self):
         return [(self._g.arc[i].a >> 32, self._g.arc[i].a & 0xffffffff, self._g.arc[i].o) for i in range(self._g.n_arc)]
 
-    def ed(self, q, v0, v1=-1, exact_start=False, max_lag=0):
-        """max_lag > 0: the product's lag pruning (GWF_F_MAX_LAG) after each step."""
+    def ed(self, q, v0, v1=-1, exact_start=False, max_lag=0, entry_key=False):
+        """max_lag > 0: the product's lag pruning (GWF_F_MAX_LAG) after each step. entry_key: the
+        product's arrival key (differs from the reference's only where the arcs into a vertex
+        carry different overlaps)."""
         b = q.encode() if isinstance(q, str) else bytes(q)
         st = Stats()
-        d = lib().gwfo_ed_lag(self.ptr, len(b), b, v0, v1, O_EXACT_START if exact_start else 0, max_lag,
-                              ctypes.byref(st))
+        opts = (O_EXACT_START if exact_start else 0) | (O_ENTRY_KEY if entry_key else 0)
+        d = lib().gwfo_ed_lag(self.ptr, len(b), b, v0, v1, opts, max_lag, ctypes.byref(st))
         return d, st
 
-    def ed_batch(self, cat, offs, lens, v0, v1=-1, exact_start=False, threads=0, stats=True):
+    def ed_batch(self, cat, offs, lens, v0, v1=-1, exact_start=False, threads=0, stats=True, entry_key=False):
         n = len(lens)
         cat = np.ascontiguousarray(cat, dtype=np.uint8)
         offs = np.ascontiguousarray(offs, dtype=np.int64)
@@ -115,8 +118,9 @@ class OracleGraph:
         dist = np.zeros(n, dtype=np.int32)
         st = (Stats * max(n, 1))() if stats else None
         used = lib().gwfo_ed_batch(self.ptr, n, cat.ctypes.data, offs.ctypes.data, lens.ctypes.data,
-                                   v0.ctypes.data, v1, O_EXACT_START if exact_start else 0, dist.ctypes.data,
-                                   st, threads)
+                                   v0.ctypes.data, v1,
+                                   (O_EXACT_START if exact_start else 0) | (O_ENTRY_KEY if entry_key else 0),
+                                   dist.ctypes.data, st, threads)
         return dist, st, used
 
     def dp(self, q, v0, v1=-1):

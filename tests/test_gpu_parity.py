@@ -65,6 +65,51 @@ def test_random_graphs_match_oracle(G, O, exact):
     assert checked > 200
 
 
+@pytest.mark.parametrize("exact", [False, True])
+@pytest.mark.parametrize("overlap", ["uniform", "mixed"])
+def test_random_graphs_with_overlaps(G, O, overlap, exact):
+    """Arcs that enter their target at a non-zero offset (GFA "nM" links): cyclic and acyclic
+    graphs, v1 targets, both forms. With one overlap per target (uniform) the kernels equal the
+    reference restatement; with different overlaps into one vertex (mixed) they equal the
+    oracle under the library's entry-keyed arrival rule, which is the DP's exact distance and
+    never above the reference's queue-order-dependent result."""
+    flags = G.GWF_F_EXACT_START if exact else 0
+    checked = 0
+    seed = 404 + 2 * (overlap == "mixed") + exact
+    for t, (seqs, arcs, v0, v1, q) in enumerate(cases(seed, 250, v1_prob=0.25, overlap=overlap)):
+        og = O.OracleGraph(seqs, arcs)
+        od, ost = og.ed(q, v0, v1, exact_start=exact, entry_key=True)
+        rd, rst = og.ed(q, v0, v1, exact_start=exact)
+        if (ost.flags | rst.flags) & O.F_NONTERM:
+            continue
+        g = _indexed(G, G.Graph.from_arrays(seqs, arcs))
+        d, st = g.ed_batch([q], [v0], v1=v1, flags=flags, mode=G.MODE_PLAIN if t % 2 else G.MODE_PERSISTENT)
+        assert st[0] == 0 and d[0] == od, (seqs, arcs, v0, v1, q, d[0], od)
+        if overlap == "uniform":
+            assert d[0] == rd
+        if exact and v1 < 0:
+            assert d[0] == og.dp(q, v0, v1) and d[0] <= rd
+        checked += 1
+        g.close()
+    assert checked > 200
+
+
+def test_lag_pruning_random_graphs_with_overlaps(G, O):
+    checked = 0
+    for t, (seqs, arcs, v0, v1, q) in enumerate(cases(921, 150, v1_prob=0.3, overlap="uniform")):
+        lag = 1 + t % 4
+        og = O.OracleGraph(seqs, arcs)
+        od, ost = og.ed(q, v0, v1, max_lag=lag)
+        if ost.flags & O.F_NONTERM:
+            continue
+        g = _indexed(G, G.Graph.from_arrays(seqs, arcs))
+        d, st = g.ed_batch([q], [v0], v1=v1, flags=G.GWF_F_MAX_LAG, max_lag=lag)
+        assert st[0] == 0 and d[0] == od, (seqs, arcs, v0, v1, q, lag, d[0], od)
+        checked += 1
+        g.close()
+    assert checked > 100
+
+
 def test_single_read_entry_point(G, O):
     w = G.load_workload("config1", n=20)
     g = _indexed(G, w["graph"])

@@ -21,6 +21,35 @@ def test_oracle_exact_start_equals_dp(O):
     assert n == 600
 
 
+def test_oracle_uniform_overlaps_equal_dp(O):
+    """Arcs entering their targets at a non-zero offset (GFA "nM" links), the same offset for
+    every arc into a vertex: the reference's arrival key (vertex, query position) names one graph
+    position, the library's entry-keyed rule gives the same result, and both equal the DP."""
+    for seqs, arcs, v0, v1, q in cases(111, 600, overlap="uniform"):
+        g = O.OracleGraph(seqs, arcs)
+        d, _ = g.ed(q, v0, -1, exact_start=True)
+        de, _ = g.ed(q, v0, -1, exact_start=True, entry_key=True)
+        assert d == de == g.dp(q, v0, -1), (seqs, arcs, v0, q)
+        for v1_ in (v1, -1):  # also with the reference's start state and with targets
+            assert g.ed(q, v0, v1_)[0] == g.ed(q, v0, v1_, entry_key=True)[0]
+
+
+def test_oracle_mixed_overlaps_entry_key_is_exact(O):
+    """Arcs into one vertex with different overlaps: the reference keys arrivals by (vertex,
+    query position), so an arrival through one arc can hide one through another that enters at a
+    different offset, and its result depends on its FIFO order (gwf-ed.cu:1196, 1106-1255). The
+    entry-keyed rule the library uses equals the DP; the reference's result is never below it."""
+    n_worse = 0
+    for seqs, arcs, v0, v1, q in cases(112, 1500, overlap="mixed"):
+        g = O.OracleGraph(seqs, arcs)
+        d, st = g.ed(q, v0, -1, exact_start=True)
+        de, _ = g.ed(q, v0, -1, exact_start=True, entry_key=True)
+        assert de == g.dp(q, v0, -1), (seqs, arcs, v0, q)
+        assert d >= de
+        n_worse += d > de
+    assert n_worse > 0  # the inputs do reach the order-dependent case
+
+
 def test_oracle_quirk_adds_cost_on_short_start_vertex(O):
     """gwf-ed.cu:809,833: k=-1 against an unsigned max_k: a start vertex shorter than 32 bases
     does not extend at s=0, so a perfect match costs 1."""
