@@ -30,6 +30,7 @@ GWF_E_BUSY = -10
 
 GWF_F_EXACT_START = 1
 GWF_F_MAX_LAG = 2
+GWF_F_BOTH_STRANDS = 4
 MODE_AUTO, MODE_PLAIN, MODE_PERSISTENT = 0, 1, 2
 
 
@@ -54,7 +55,7 @@ class GwfGraph(ctypes.Structure):
 
 class BatchOpts(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int32), ("flags", ctypes.c_int32), ("device", ctypes.c_int32),
-                ("warps_per_cta", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
+                ("warps_per_read", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
                 ("use_graph", ctypes.c_int32), ("reserved", ctypes.c_int32 * 10)]
 
 
@@ -81,6 +82,7 @@ SIGNATURES = {
     "gwf_ed": (I32, [P, PG, I32, ctypes.c_char_p, I32, I32, U32, I32]),
     "gwf_ed_batch": (ctypes.c_int, [PG, I32, P, P, P, I32, U32, P, P, P]),
     "gwf_ed_batch_concat": (ctypes.c_int, [PG, I32, P, P, P, P, I32, U32, P, P, P]),
+    "gwf_ed_batch_strand": (ctypes.c_int, [PG, I32, P, P, P, P, I32, U32, P, P, P, P]),
     "gwf_ed_batch_path": (ctypes.c_int, [PG, I32, P, P, P, P, I32, I32, I32, P, P, P, P, P, P]),
     "gwf_reads_load": (ctypes.POINTER(GwfReads), [ctypes.c_char_p]),
     "gwf_reads_free": (None, [ctypes.POINTER(GwfReads)]),
@@ -95,6 +97,7 @@ SIGNATURES = {
     "gwf_tune": (ctypes.c_int, [PG, I32, P, P, P, P, I32, I32, ctypes.c_char_p]),
     "gwf_tune_load": (ctypes.c_int, [ctypes.c_char_p, I32]),
     "gwf_tune_get": (ctypes.c_int, [I32, I32, P, P, P]),
+    "gwf_tune_get_shape": (ctypes.c_int, [I32, I32, P, P, P, P]),
     "gwf_tune_clear": (None, [I32]),
     "gwf_pinned_alloc": (P, [I64]),
     "gwf_pinned_free": (None, [P]),
@@ -103,6 +106,7 @@ SIGNATURES = {
     "gwf_srv_poll": (ctypes.c_int, [P, I64, P, P]),
     "gwf_srv_wait": (ctypes.c_int, [P, I64, P, P, DBL]),
     "gwf_srv_times": (ctypes.c_int, [P, I64, P, P, P]),
+    "gwf_srv_strand": (ctypes.c_int, [P, I64, P]),
     "gwf_srv_stats": (ctypes.c_int, [P, P, I32]),
     "gwf_srv_destroy": (None, [P]),
     "gwf_gfa_load": (PG, [ctypes.c_char_p, ctypes.c_char_p]),
@@ -290,8 +294,11 @@ class Graph:
             raise GwfError(r, last_error())
         return r
 
-    def ed_batch(self, reads, v0, v1=-1, mode=MODE_AUTO, flags=0, concat=True, max_lag=0, use_graph=0):
-        """Batch alignment. reads: list of bytes, or (cat, offs, lens). Returns (dist, status)."""
+    def ed_batch(self, reads, v0, v1=-1, mode=MODE_AUTO, flags=0, concat=True, max_lag=0, use_graph=0,
+                 warps_per_read=0):
+        """Batch alignment. reads: list of bytes, or (cat, offs, lens). Returns (dist, status).
+        warps_per_read: 1, 2, 4 or 8 warps align each read of the persistent form (0 = per
+        length bucket: tuned for MODE_AUTO, else the library's default)."""
         if isinstance(reads, tuple):
             cat, offs, lens = reads
         else:
@@ -300,7 +307,7 @@ class Graph:
         v0 = np.ascontiguousarray(np.broadcast_to(np.asarray(v0, dtype=np.int32), (n,)))
         dist = np.zeros(n, dtype=np.int32)
         st = np.zeros(n, dtype=np.int32)
-        opt = BatchOpts(mode=mode, flags=flags, use_graph=use_graph)
+        opt = BatchOpts(mode=mode, flags=flags, use_graph=use_graph, warps_per_read=warps_per_read)
         if concat:
             rc = lib().gwf_ed_batch_concat(self.ptr, n, _ptr(cat), _ptr(offs), _ptr(lens), _ptr(v0), v1,
                                            max_lag, _ptr(dist), _ptr(st), ctypes.byref(opt))
@@ -311,6 +318,21 @@ class Graph:
         if rc != 0:
             raise GwfError(rc, last_error())
         return dist, st
+
+    def ed_strand(self, reads, v0, v1=-1, mode=MODE_AUTO, flags=0, max_lag=0, use_graph=0, warps_per_read=0):
+        """Both-strand alignment (gwf_ed_batch_strand): each read and its reverse complement from
+        v0. Returns (dist, status, strand), strand 0 = as given, 1 = reverse complement, -1 =
+        none."""
+        cat, offs, lens = reads if isinstance(reads, tuple) else pack_reads(reads)
+        n = len(lens)
+        v0 = np.ascontiguousarray(np.broadcast_to(np.asarray(v0, dtype=np.int32), (n,)))
+        dist, st, strand = (np.zeros(n, dtype=np.int32) for _ in range(3))
+        opt = BatchOpts(mode=mode, flags=flags, use_graph=use_graph, warps_per_read=warps_per_read)
+        rc = lib().gwf_ed_batch_strand(self.ptr, n, _ptr(cat), _ptr(offs), _ptr(lens), _ptr(v0), v1, max_lag,
+                                       _ptr(dist), _ptr(st), _ptr(strand), ctypes.byref(opt))
+        if rc != 0:
+            raise GwfError(rc, last_error())
+        return dist, st, strand
 
     def ed_path(self, reads, v0, v1=-1, flags=0, max_nv=4096, as_arrays=False, max_ops=0):
         """Alignment with traceback (gwf_ed_batch_path; gwf_ed_batch_align when max_ops > 0).
@@ -433,13 +455,15 @@ def tune_load(json_path, device=-1):
     return tune_table(device)
 
 
-def tune_table(device=-1):
-    """{bucket: (form, ctas_per_sm, reads_per_s)} for the buckets with an entry."""
+def tune_table(device=-1, with_warps=False):
+    """{bucket: (form, ctas_per_sm, reads_per_s)} for the buckets with an entry; with_warps=True
+    adds the bucket's warps per read: (form, ctas_per_sm, warps_per_read, reads_per_s)."""
     out = {}
     for b in range(len(TUNE_BUCKET_MAX)):
-        f, c, r = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_float()
-        if lib().gwf_tune_get(device, b, ctypes.byref(f), ctypes.byref(c), ctypes.byref(r)) == 1:
-            out[b] = (f.value, c.value, r.value)
+        f, c, nw, r = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_float()
+        if lib().gwf_tune_get_shape(device, b, ctypes.byref(f), ctypes.byref(c), ctypes.byref(nw),
+                                    ctypes.byref(r)) == 1:
+            out[b] = (f.value, c.value, nw.value, r.value) if with_warps else (f.value, c.value, r.value)
     return out
 
 
@@ -460,10 +484,10 @@ class ResidentBatch:
         if not self.ptr:
             raise GwfError(GWF_E_CUDA, last_error())
 
-    def run(self, mode=None, flags=None, ctas_per_sm=0, use_graph=0):
+    def run(self, mode=None, flags=None, ctas_per_sm=0, use_graph=0, warps_per_read=0):
         opt = BatchOpts(mode=self.opt.mode if mode is None else mode,
                         flags=self.opt.flags if flags is None else flags, ctas_per_sm=ctas_per_sm,
-                        use_graph=use_graph)
+                        use_graph=use_graph, warps_per_read=warps_per_read)
         ms = ctypes.c_float(0)
         rc = lib().gwf_batch_run(self.ptr, ctypes.byref(opt), ctypes.byref(ms))
         if rc != 0:
@@ -535,6 +559,14 @@ class Server:
         if rc < 0:
             raise GwfError(rc, last_error())
         return (dist, st) if rc == 1 else None
+
+    def strand(self, rid, n):
+        """Strand per read of a finished request of a both-strand server (GWF_F_BOTH_STRANDS)."""
+        out = np.zeros(n, dtype=np.int32)
+        rc = lib().gwf_srv_strand(self.ptr, rid, _ptr(out))
+        if rc != 0:
+            raise GwfError(rc, last_error())
+        return out
 
     def times(self, rid):
         a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()

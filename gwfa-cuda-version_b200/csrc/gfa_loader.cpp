@@ -909,6 +909,8 @@ gwf_graph_t *load_text(const char *text, size_t len, const char *start_seg)
 
 } // namespace
 
+unsigned char gwf_comp_base(unsigned char c) { return comp_base(c); }
+
 // The whole (decompressed) file in one malloc'd buffer; realloc grows it without filling it.
 // "-" or NULL is standard input. Returns NULL (and sets the error) on failure.
 char *gwf_read_file(const char *path, size_t *len)

@@ -2,7 +2,7 @@
 // (main.cu:360-750): the same options and arguments, one edit distance per read on stdout, in
 // input order. The alignment runs through the library's batch entry point on the device.
 //
-//   gwf-b200 [-p] [-s STR] [-l INT [-P]] [-m persistent|plain] [-x] [-t] <target.gfa> <query.fa|fq[.gz]>
+//   gwf-b200 [-p] [-s STR] [-l INT [-P]] [-m persistent|plain] [-x] [-t | -b] <target.gfa> <query.fa|fq[.gz]>
 //
 //   -p   print the graph (gwf_graph_print format) and exit     (main.cu:382-387, 354-359)
 //   -s   starting segment name [first]; a trailing + or - picks the strand (main.cu:399-407)
@@ -13,6 +13,9 @@
 //   -t   traceback: after each distance, the end offset, the vertex path and the CIGAR of the
 //        read against the path's text (no reference counterpart; the reference's traceback
 //        argument is unused, README.md:117-118)
+//   -b   both strands: each read and its reverse complement; prints the smaller distance and
+//        + (the read as given) or - (its reverse complement) (GWF_F_BOTH_STRANDS; the reference
+//        aligns the read as given only, main.cu:370, 404)
 //
 // Every read is aligned from offset 0 of the start segment (vertex 0 of the converted graph),
 // as the reference kernel does (main.cu:217). Timing and counts go to stderr.
@@ -40,13 +43,14 @@ void usage()
 	fprintf(stderr, "  -m STR    execution form: persistent or plain [persistent]\n");
 	fprintf(stderr, "  -x        exact start state (no reference start-state rule)\n");
 	fprintf(stderr, "  -t        traceback: print distance, end offset, vertex path and CIGAR per read\n");
+	fprintf(stderr, "  -b        both strands: print distance and + or - (the read or its reverse complement)\n");
 }
 
 } // namespace
 
 int main(int argc, char *argv[])
 {
-	bool print_graph = false, exact = false, trace = false, prune = false;
+	bool print_graph = false, exact = false, trace = false, prune = false, both = false;
 	const char *sname = nullptr;
 	int32_t mode = GWF_MODE_PERSISTENT;
 	uint32_t max_lag = 0;
@@ -57,6 +61,7 @@ int main(int argc, char *argv[])
 		else if (!strcmp(a, "-x")) exact = true;
 		else if (!strcmp(a, "-t")) trace = true;
 		else if (!strcmp(a, "-P")) prune = true;
+		else if (!strcmp(a, "-b")) both = true;
 		else if (!strcmp(a, "-s") && i + 1 < argc) sname = argv[++i];
 		else if (!strcmp(a, "-l") && i + 1 < argc) max_lag = (uint32_t)atoi(argv[++i]);
 		else if (!strcmp(a, "-m") && i + 1 < argc) {
@@ -72,7 +77,7 @@ int main(int argc, char *argv[])
 			return 1;
 		}
 	}
-	if ((!print_graph && argc - i < 2) || (print_graph && argc - i < 1)) {
+	if ((!print_graph && argc - i < 2) || (print_graph && argc - i < 1) || (both && trace)) {
 		usage();
 		return 1;
 	}
@@ -113,7 +118,7 @@ int main(int argc, char *argv[])
 	fprintf(stderr, "[gwf-b200] %d reads, %lld bases, %u vertices, %u arcs\n", n, (long long)rs->n_bases, g->n_vtx,
 	        g->n_arc);
 	gwf_ed_index(g);
-	std::vector<int32_t> v0((size_t)n, 0), dist((size_t)n, -1), status((size_t)n, 0);
+	std::vector<int32_t> v0((size_t)n, 0), dist((size_t)n, -1), status((size_t)n, 0), strand((size_t)n, -1);
 	gwf_batch_opts_t opt;
 	memset(&opt, 0, sizeof opt);
 	opt.mode = mode;
@@ -159,6 +164,9 @@ int main(int argc, char *argv[])
 				}
 			}
 		}
+	} else if (n > 0 && both) {
+		rc = gwf_ed_batch_strand(g, n, cat, offs.data(), lens.data(), v0.data(), -1, max_lag, dist.data(),
+		                         status.data(), strand.data(), &opt);
 	} else if (n > 0) {
 		rc = gwf_ed_batch_concat(g, n, cat, offs.data(), lens.data(), v0.data(), -1, max_lag, dist.data(),
 		                         status.data(), &opt);
@@ -173,6 +181,7 @@ int main(int argc, char *argv[])
 	int32_t bad = 0;
 	for (int32_t j = 0; j < n; ++j) {
 		if (trace) printf("%d%s\n", dist[(size_t)j], paths[(size_t)j].c_str());
+		else if (both) printf("%d\t%c\n", dist[(size_t)j], strand[(size_t)j] == 1 ? '-' : strand[(size_t)j] == 0 ? '+' : '*');
 		else printf("%d\n", dist[(size_t)j]);
 		if (status[(size_t)j] != GWF_OK) ++bad;
 	}

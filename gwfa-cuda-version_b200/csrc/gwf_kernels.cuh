@@ -1024,6 +1024,55 @@ __global__ void __launch_bounds__(256, 3) k_serve(const __grid_constant__ SrvPar
 	}
 }
 
+// IUPAC complement (upper and lower case; other bytes map to themselves), as the GFA loader
+// complements reverse-strand segments.
+__device__ __forceinline__ uint8_t comp_byte(uint8_t c)
+{
+	switch (c) {
+	case 'A': return 'T';
+	case 'T': return 'A';
+	case 'C': return 'G';
+	case 'G': return 'C';
+	case 'a': return 't';
+	case 't': return 'a';
+	case 'c': return 'g';
+	case 'g': return 'c';
+	case 'R': return 'Y';
+	case 'Y': return 'R';
+	case 'K': return 'M';
+	case 'M': return 'K';
+	case 'B': return 'V';
+	case 'V': return 'B';
+	case 'D': return 'H';
+	case 'H': return 'D';
+	case 'r': return 'y';
+	case 'y': return 'r';
+	case 'k': return 'm';
+	case 'm': return 'k';
+	case 'b': return 'v';
+	case 'v': return 'b';
+	case 'd': return 'h';
+	case 'h': return 'd';
+	case 'U': return 'A';
+	case 'u': return 'a';
+	default: return c;
+	}
+}
+
+// Both strands: read n + r (at raw_off[n + r]) becomes the reverse complement of read r. One
+// warp per read.
+__global__ void __launch_bounds__(256) k_revcomp_reads(uint8_t *__restrict__ raw, const int64_t *__restrict__ raw_off,
+                                                       const int32_t *__restrict__ ql, int32_t n)
+{
+	const int lane = threadIdx.x & 31;
+	const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+	if (r >= n) return;
+	const uint8_t *src = raw + raw_off[r];
+	uint8_t *dst = raw + raw_off[n + r];
+	const int32_t L = ql[r] > 0 ? ql[r] : 0;
+	for (int32_t i = lane; i < L; i += 32) dst[L - 1 - i] = comp_byte(src[i]);
+}
+
 // Packs reads to 2 bits per base (A=0 C=1 T=2 G=3 from bits 1-2 of the ASCII code) and flags
 // reads that contain anything but A/C/G/T. One warp per read; lane l builds words l, l+32, ...
 __global__ void __launch_bounds__(256) k_pack_reads(const uint8_t *__restrict__ raw,

@@ -18,6 +18,7 @@
 
 #include "../../include/gwfa.h"
 #include "gwf_cigar.cuh"
+#include "gwf_group.cuh"
 #include "gwf_kernels.cuh"
 #include "gwf_runtime.h"
 #include "gwfa_internal.h"
@@ -338,6 +339,9 @@ Engine *gwf_engine(int dev)
 	int occ = 0;
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_align_persistent, 256, 0);
 	E->persistent_ctas_per_sm = occ > 0 ? occ : 1;
+	occ = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_align_classes, 256, 0);
+	E->classes_ctas_per_sm = occ > 0 ? occ : 1;
 	g_engines[dev] = E;
 	return E;
 }
@@ -345,8 +349,9 @@ Engine *gwf_engine(int dev)
 // ------------------------------------------------------------------ batches
 void Batch::release()
 {
-	for (DBuf *b : {&raw, &raw_off, &ql, &v0, &pk, &pk_off, &pure, &dist, &status, &steps, &order_ql})
+	for (DBuf *b : {&raw, &raw_off, &ql, &v0, &pk, &pk_off, &pure, &dist, &status, &steps, &order_ql, &order_cls})
 		b->release();
+	cls_key = ~0ULL;
 	h_meta.release();
 	if (gexec) cudaGraphExecDestroy(gexec), gexec = nullptr;
 }
@@ -356,6 +361,8 @@ void Batch::release()
 // Host-to-device copy on the engine's stream. A page-locked source goes to the DMA engine as
 // it is; a pageable one of more than 1 MiB passes through two pinned 8 MiB chunks in turn, so
 // that filling one chunk overlaps the transfer of the other.
+static const int kWarpsPerCtaPack = 8; // warps per CTA of the per-read helper kernels
+
 static int upload(Engine &E, void *dst, const void *src, size_t n)
 {
 	cudaPointerAttributes at;
@@ -379,27 +386,36 @@ static int upload(Engine &E, void *dst, const void *src, size_t n)
 	return 0;
 }
 
-int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64_t *offs,
-                   const int32_t *ql, const int32_t *v0, int32_t v1)
+int gwf_batch_load(Engine &E, Batch &B, int32_t n_in, const char *seqs, const int64_t *offs,
+                   const int32_t *ql_in, const int32_t *v0, int32_t v1, bool both)
 {
-	B.n = n, B.v1 = v1;
+	// with both strands the batch holds 2 n reads: read n + i is the reverse complement of read
+	// i, made on the device, with the same v0
+	const int32_t n = both ? 2 * n_in : n_in;
+	if (both && n_in > INT32_MAX / 2) return GWF_E_BAD_INPUT;
+	B.n = n, B.n_in = n_in, B.both = both, B.v1 = v1;
 	++B.generation;
-	B.h_ql.assign(ql, ql + n);
+	B.h_ql.assign(ql_in, ql_in + n_in);
+	if (both) B.h_ql.insert(B.h_ql.end(), ql_in, ql_in + n_in);
+	const int32_t *ql = B.h_ql.data();
 	int64_t lo = 0, hi = 0;
-	if (n > 0) {
+	if (n_in > 0) {
 		lo = offs[0], hi = offs[0];
-		for (int32_t i = 0; i < n; ++i) {
+		for (int32_t i = 0; i < n_in; ++i) {
 			if (ql[i] < 0) return GWF_E_BAD_INPUT;
 			lo = std::min(lo, offs[i]);
 			hi = std::max(hi, offs[i] + ql[i]);
 		}
 	}
+	const int64_t span = hi - lo, rc_base = span + 16; // the reverse complements after the reads
 	// pinned metadata: raw offsets and packed offsets (int64), queue order (int32)
 	int rc;
 	if ((rc = B.h_meta.ensure(20 * (size_t)n + 64))) return rc;
 	int64_t *h_raw_off = (int64_t *)B.h_meta.p, *h_pk_off = h_raw_off + n;
 	int32_t *h_order = (int32_t *)(h_pk_off + n);
-	for (int32_t i = 0; i < n; ++i) h_raw_off[i] = offs[i] - lo;
+	for (int32_t i = 0; i < n_in; ++i) h_raw_off[i] = offs[i] - lo;
+	if (both)
+		for (int32_t i = 0; i < n_in; ++i) h_raw_off[n_in + i] = rc_base + offs[i] - lo;
 	int64_t words = 0;
 	for (int32_t i = 0; i < n; ++i) h_pk_off[i] = words, words += (ql[i] + 31) / 32 + 2;
 	B.pk_words = words;
@@ -419,7 +435,7 @@ int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64
 		for (int32_t b = 0; b < nb; ++b) cnt[(size_t)b + 1] += cnt[(size_t)b];
 		for (int32_t i = 0; i < n; ++i) h_order[cnt[(size_t)(nb - 1 - (ql[i] >> 6))]++] = i;
 	}
-	const size_t nraw = (size_t)(hi - lo) + 16;
+	const size_t nraw = (size_t)(both ? 2 * rc_base : rc_base);
 	if ((rc = B.raw.ensure(nraw)) || (rc = B.raw_off.ensure(8 * (size_t)n + 8)) ||
 	    (rc = B.ql.ensure(4 * (size_t)n + 4)) || (rc = B.v0.ensure(4 * (size_t)n + 4)) ||
 	    (rc = B.pk.ensure(8 * (size_t)words + 8)) || (rc = B.pk_off.ensure(8 * (size_t)n + 8)) ||
@@ -429,15 +445,42 @@ int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64
 		return rc;
 	cudaStream_t s = E.stream;
 	if (n > 0) {
-		if ((rc = upload(E, B.raw.p, seqs + lo, (size_t)(hi - lo)))) return rc;
-		CK(cudaMemsetAsync((char *)B.raw.p + (hi - lo), 0, 16, s));
+		if ((rc = upload(E, B.raw.p, seqs + lo, (size_t)span))) return rc;
+		CK(cudaMemsetAsync((char *)B.raw.p + span, 0, 16, s));
 		CK(cudaMemcpyAsync(B.raw_off.p, h_raw_off, 8 * (size_t)n, cudaMemcpyHostToDevice, s));
-		if ((rc = upload(E, B.ql.p, ql, 4 * (size_t)n)) || (rc = upload(E, B.v0.p, v0, 4 * (size_t)n)))
+		if ((rc = upload(E, B.ql.p, ql_in, 4 * (size_t)n_in)) || (rc = upload(E, B.v0.p, v0, 4 * (size_t)n_in)))
 			return rc;
+		if (both) {
+			CK(cudaMemcpyAsync((int32_t *)B.ql.p + n_in, B.ql.p, 4 * (size_t)n_in, cudaMemcpyDeviceToDevice, s));
+			CK(cudaMemcpyAsync((int32_t *)B.v0.p + n_in, B.v0.p, 4 * (size_t)n_in, cudaMemcpyDeviceToDevice, s));
+			CK(cudaMemsetAsync((char *)B.raw.p + rc_base + span, 0, 16, s));
+			const int ctas = (n_in + kWarpsPerCtaPack - 1) / kWarpsPerCtaPack;
+			k_revcomp_reads<<<ctas, 32 * kWarpsPerCtaPack, 0, s>>>((uint8_t *)B.raw.p, (const int64_t *)B.raw_off.p,
+			                                                      (const int32_t *)B.ql.p, n_in);
+			CK(cudaGetLastError());
+		}
 		CK(cudaMemcpyAsync(B.pk_off.p, h_pk_off, 8 * (size_t)n, cudaMemcpyHostToDevice, s));
 		CK(cudaMemcpyAsync(B.order_ql.p, h_order, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
 	}
 	return 0;
+}
+
+// Both strands: read i's result from its two strands (i and n_in + i). The smaller distance
+// wins, the read itself on a tie; a strand that did not finish (a non-OK status) makes the read's
+// status that status and its distance -1.
+static void combine_strands(int32_t n_in, const int32_t *d2, const int32_t *s2, int32_t *dist, int32_t *status,
+                            int32_t *strand)
+{
+	for (int32_t i = 0; i < n_in; ++i) {
+		const int32_t df = d2[i], dr = d2[n_in + i], sf = s2[i], sr = s2[n_in + i];
+		int32_t d = -1, st = GWF_OK, k = -1;
+		if (sf != GWF_OK || sr != GWF_OK) st = sf != GWF_OK ? sf : sr;
+		else if (df >= 0 && (dr < 0 || df <= dr)) d = df, k = 0;
+		else if (dr >= 0) d = dr, k = 1;
+		if (dist) dist[i] = d;
+		if (status) status[i] = st;
+		if (strand) strand[i] = k;
+	}
 }
 
 static DevReads reads_view(const Batch &B)
@@ -585,24 +628,132 @@ static int enqueue_pack(Engine &E, Batch &B)
 	return 0;
 }
 
+// ---- read classes: reads aligned by groups of 2, 4 or 8 warps
+//
+// Each read gets a number of warps from its length bucket (the caller's forced value, the tuned
+// table, or gwf_default_nw). The reads of one count form a class; classes run longest reads
+// first (8, 4, 2, then 1 warp per read), each class's queue ordered longest read first. One
+// launch of k_align_classes runs all classes.
+const int32_t gwf_default_nw[GWF_TUNE_NBUCKETS] = {1, 1, 1, 1, 1};
+static const int32_t kClassNw[4] = {8, 4, 2, 1};
+
+// Class layout of the batch for the per-bucket warp counts nw_b; uploads the class queues when
+// the layout changed. Returns the number of classes with reads.
+static int plan_classes(Engine &E, Batch &B, const int32_t *nw_b)
+{
+	uint64_t key = B.generation << 20;
+	for (int b = 0; b < GWF_TUNE_NBUCKETS; ++b) key |= (uint64_t)(nw_b[b] & 15) << (4 * b);
+	if (key == B.cls_key) return 0;
+	int32_t cls_of_bucket[GWF_TUNE_NBUCKETS];
+	for (int b = 0; b < GWF_TUNE_NBUCKETS; ++b) {
+		cls_of_bucket[b] = 3;
+		for (int k = 0; k < 4; ++k)
+			if (kClassNw[k] == nw_b[b]) cls_of_bucket[b] = k;
+	}
+	int32_t cnt[4] = {0, 0, 0, 0}, cap[4] = {0, 0, 0, 0};
+	std::vector<uint8_t> cls((size_t)B.n);
+	for (int32_t i = 0; i < B.n; ++i) {
+		const int32_t q = B.h_ql[(size_t)i];
+		const int k = cls_of_bucket[gwf_tune_bucket(q)];
+		cls[(size_t)i] = (uint8_t)k, ++cnt[k], cap[k] = std::max(cap[k], q);
+	}
+	// each class longest read first: counting sort over 64-base length buckets
+	std::vector<int32_t> order((size_t)B.n);
+	int32_t start[4], pos = 0;
+	for (int k = 0; k < 4; ++k) start[k] = pos, pos += cnt[k];
+	const int32_t nb = (B.max_ql >> 6) + 1;
+	std::vector<int32_t> c2((size_t)(4 * nb + 1), 0);
+	for (int32_t i = 0; i < B.n; ++i)
+		c2[(size_t)(cls[(size_t)i] * nb + (nb - 1 - (B.h_ql[(size_t)i] >> 6))) + 1]++;
+	for (size_t b = 0; b + 1 < c2.size(); ++b) c2[b + 1] += c2[b];
+	for (int32_t i = 0; i < B.n; ++i)
+		order[(size_t)c2[(size_t)(cls[(size_t)i] * nb + (nb - 1 - (B.h_ql[(size_t)i] >> 6)))]++] = i;
+	int rc;
+	if ((rc = B.order_cls.ensure(4 * (size_t)B.n + 4))) return rc;
+	CK(cudaMemcpyAsync(B.order_cls.p, order.data(), 4 * (size_t)B.n, cudaMemcpyHostToDevice, E.stream));
+	CK(cudaStreamSynchronize(E.stream)); // the host order vector goes out of scope
+	B.cls_n = 0;
+	for (int k = 0; k < 4; ++k)
+		if (cnt[k] > 0) {
+			const int j = B.cls_n++;
+			B.cls_nw[j] = kClassNw[k], B.cls_cnt[j] = cnt[k], B.cls_cap[j] = cap[k], B.cls_start[j] = start[k];
+		}
+	B.cls_key = key;
+	return 0;
+}
+
+// Grid and arena of a class launch: a CTA holds, for the class that needs most, 8 / nw group
+// arenas sized for the class's longest read; as many CTAs as the budget and the reads allow.
+struct ClassLaunch {
+	ClassParams cp;
+	int ctas = 0;
+};
+
+static int plan_class_launch(Engine &E, const Batch &B, int ctas_per_sm, int32_t dens_milli, ClassLaunch *cl)
+{
+	ClassParams &cp = cl->cp;
+	memset(&cp, 0, sizeof cp);
+	int64_t need_ctas = 0;
+	cp.cta_bytes = 0;
+	for (int j = 0; j < B.cls_n; ++j) {
+		const int groups = 8 / B.cls_nw[j];
+		cp.order[j] = (const int32_t *)B.order_cls.p + B.cls_start[j];
+		cp.n[j] = B.cls_cnt[j], cp.nw[j] = B.cls_nw[j], cp.ql_cap[j] = B.cls_cap[j];
+		cp.slot[j] = ws_layout(caps_for(B.cls_cap[j], 0, dens_milli)).total;
+		cp.cta_bytes = std::max<int64_t>(cp.cta_bytes, groups * cp.slot[j]);
+		need_ctas = std::max<int64_t>(need_ctas, ((int64_t)B.cls_cnt[j] + groups - 1) / groups);
+	}
+	cp.n_cls = B.cls_n;
+	int64_t ctas = std::min<int64_t>((int64_t)E.sm_count * ctas_per_sm, std::max<int64_t>(1, need_ctas));
+	const int64_t budget = std::max<int64_t>(E.mem_budget, (int64_t)E.ws.cap);
+	while (ctas > 1 && ctas * cp.cta_bytes > budget) --ctas;
+	if (ctas * cp.cta_bytes > budget) {
+		gwf_set_errorf("arena of %lld bytes per CTA does not fit the device", (long long)cp.cta_bytes);
+		return GWF_E_NOMEM;
+	}
+	int rc;
+	if ((rc = E.ws.ensure((size_t)(ctas * cp.cta_bytes)))) return rc;
+	if ((rc = E.head.ensure(16))) return rc;
+	cp.head = (int32_t *)E.head.p;
+	cl->ctas = (int)ctas;
+	return 0;
+}
+
+static int enqueue_classes(Engine &E, KParams p, const ClassLaunch &cl)
+{
+	CK(cudaMemsetAsync(E.head.p, 0, 16, E.stream));
+	p.ws = (uint8_t *)E.ws.p;
+	p.level = 0;
+	k_align_classes<<<cl.ctas, 32 * kWarpsPerCta, 0, E.stream>>>(p, cl.cp);
+	CK(cudaGetLastError());
+	return 0;
+}
+
 // Level-0 sequence of the persistent form as one CUDA graph: pack, clear the overflow count,
 // persistent kernel, copy the overflow count to the host. Captured once per batch contents and
 // launch shape, replayed on every run.
-static int launch_level0_graph(Engine &E, Batch &B, const KParams &p, int ctas_per_sm)
+static int launch_level0_graph(Engine &E, Batch &B, const KParams &p, int ctas_per_sm, bool classes)
 {
 	PersistPlan pl;
+	ClassLaunch cl;
 	int rc;
-	if ((rc = plan_persistent(E, B.n, B.max_ql, 0, ctas_per_sm, p.dens_milli, &pl))) return rc;
-	const uint64_t key[8] = {B.generation, (uint64_t)(uintptr_t)E.ws.p, (uint64_t)pl.slot, (uint64_t)pl.ctas,
+	if (classes) {
+		if ((rc = plan_class_launch(E, B, ctas_per_sm, p.dens_milli, &cl))) return rc;
+		pl.ctas = cl.ctas, pl.slot = cl.cp.cta_bytes;
+	} else if ((rc = plan_persistent(E, B.n, B.max_ql, 0, ctas_per_sm, p.dens_milli, &pl)))
+		return rc;
+	const uint64_t key[9] = {B.generation, (uint64_t)(uintptr_t)E.ws.p, (uint64_t)pl.slot, (uint64_t)pl.ctas,
 	                         (uint64_t)(uint32_t)p.flags | (uint64_t)(uint32_t)p.max_lag << 32,
 	                         (uint64_t)(uintptr_t)E.retry_n.p,
-	                         (uint64_t)(uintptr_t)E.h_small.p, (uint64_t)(uintptr_t)E.retry_list.p};
+	                         (uint64_t)(uintptr_t)E.h_small.p, (uint64_t)(uintptr_t)E.retry_list.p,
+	                         classes ? B.cls_key : ~0ULL};
 	if (!B.gexec || memcmp(key, B.gkey, sizeof key) != 0) {
 		if (B.gexec) cudaGraphExecDestroy(B.gexec), B.gexec = nullptr;
 		CK(cudaStreamBeginCapture(E.stream, cudaStreamCaptureModeThreadLocal));
 		int erc = enqueue_pack(E, B);
 		if (!erc && cudaMemsetAsync(E.retry_n.p, 0, 4, E.stream) != cudaSuccess) erc = GWF_E_CUDA;
-		if (!erc) erc = enqueue_persistent(E, p, pl, (const int32_t *)B.order_ql.p, B.n, B.max_ql, 0);
+		if (!erc) erc = classes ? enqueue_classes(E, p, cl)
+		                        : enqueue_persistent(E, p, pl, (const int32_t *)B.order_ql.p, B.n, B.max_ql, 0);
 		if (!erc && cudaMemcpyAsync(E.h_small.p, E.retry_n.p, 4, cudaMemcpyDeviceToHost, E.stream) != cudaSuccess)
 			erc = GWF_E_CUDA;
 		cudaGraph_t graph = nullptr;
@@ -628,7 +779,8 @@ static int launch_level0_graph(Engine &E, Batch &B, const KParams &p, int ctas_p
 }
 
 int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t flags,
-                   int ctas_per_sm, float *ms, int *launches_out, int use_graph, int32_t max_lag)
+                   int ctas_per_sm, float *ms, int *launches_out, int use_graph, int32_t max_lag,
+                   int32_t warps_per_read)
 {
 	int launches = 0, rc;
 	if (B.n == 0) {
@@ -641,15 +793,28 @@ int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t
 		return rc;
 	KParams p = base_params(E, G, B, flags);
 	p.max_lag = max_lag > 0 ? max_lag : 0;
+	// warps per read of each length bucket (persistent form): forced, tuned (GWF_MODE_AUTO), or
+	// the library's defaults
+	int32_t nw_b[GWF_TUNE_NBUCKETS];
+	bool classes = false;
+	for (int b = 0; b < GWF_TUNE_NBUCKETS; ++b) {
+		int32_t nw = warps_per_read > 0 ? warps_per_read : 0;
+		if (!nw && mode == GWF_MODE_AUTO) nw = gwf_tune_lookup_nw(E.device, b);
+		if (!nw) nw = gwf_default_nw[b];
+		nw_b[b] = nw;
+		classes |= nw > 1;
+	}
 	if (mode == GWF_MODE_AUTO && ctas_per_sm <= 0) { // autotuned shape for the dominant length bucket
 		int32_t f = 0, c = 0;
 		if (gwf_tune_lookup(E.device, B.dom_bucket, &f, &c)) mode = f, ctas_per_sm = c;
 	}
-	if (ctas_per_sm <= 0) ctas_per_sm = E.persistent_ctas_per_sm;
+	classes = classes && mode != GWF_MODE_PLAIN;
+	if (classes && (rc = plan_classes(E, B, nw_b))) return rc;
+	if (ctas_per_sm <= 0) ctas_per_sm = classes ? E.classes_ctas_per_sm : E.persistent_ctas_per_sm;
 	bool count_copied = false;
 	CK(cudaEventRecord(E.ev0, E.stream));
 	if (use_graph && mode != GWF_MODE_PLAIN) {
-		if ((rc = launch_level0_graph(E, B, p, ctas_per_sm))) return rc;
+		if ((rc = launch_level0_graph(E, B, p, ctas_per_sm, classes))) return rc;
 		launches += 2;
 		count_copied = true;
 	} else {
@@ -657,7 +822,12 @@ int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t
 		++launches;
 		CK(cudaMemsetAsync(E.retry_n.p, 0, 4, E.stream));
 		if (mode == GWF_MODE_PLAIN) rc = launch_plain(E, p, B, &launches);
-		else rc = launch_persistent(E, p, (const int32_t *)B.order_ql.p, B.n, B.max_ql, 0, ctas_per_sm, &launches);
+		else if (classes) {
+			ClassLaunch cl;
+			if (!(rc = plan_class_launch(E, B, ctas_per_sm, p.dens_milli, &cl)) && !(rc = enqueue_classes(E, p, cl)))
+				++launches;
+		} else
+			rc = launch_persistent(E, p, (const int32_t *)B.order_ql.p, B.n, B.max_ql, 0, ctas_per_sm, &launches);
 		if (rc) return rc;
 	}
 	// re-run arena overflows at larger size classes
@@ -680,7 +850,8 @@ int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t
 		CK(cudaMemsetAsync(E.retry_n.p, 0, 4, E.stream));
 		KParams q = p;
 		if (level == kMaxLevel) q.retry_list = nullptr; // last class: keep GWF_E_CAPACITY
-		if ((rc = launch_persistent(E, q, (const int32_t *)E.order.p, nr, cap, level, ctas_per_sm, &launches)))
+		if ((rc = launch_persistent(E, q, (const int32_t *)E.order.p, nr, cap, level,
+		                            std::min(ctas_per_sm, E.persistent_ctas_per_sm), &launches)))
 			return rc;
 	}
 	CK(cudaEventRecord(E.ev1, E.stream));
@@ -690,18 +861,24 @@ int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t
 	return 0;
 }
 
-int gwf_batch_fetch(Engine &E, Batch &B, int32_t *dist, int32_t *status)
+int gwf_batch_fetch(Engine &E, Batch &B, int32_t *dist, int32_t *status, int32_t *strand)
 {
 	if (B.n == 0) return 0;
 	// through the pinned metadata buffer (its upload has completed: the stream is in order)
 	int rc;
 	if ((rc = B.h_meta.ensure(8 * (size_t)B.n + 64))) return rc;
 	int32_t *hd = (int32_t *)B.h_meta.p, *hs = hd + B.n;
-	if (dist) CK(cudaMemcpyAsync(hd, B.dist.p, 4 * (size_t)B.n, cudaMemcpyDeviceToHost, E.stream));
-	if (status) CK(cudaMemcpyAsync(hs, B.status.p, 4 * (size_t)B.n, cudaMemcpyDeviceToHost, E.stream));
+	if (dist || B.both) CK(cudaMemcpyAsync(hd, B.dist.p, 4 * (size_t)B.n, cudaMemcpyDeviceToHost, E.stream));
+	if (status || B.both) CK(cudaMemcpyAsync(hs, B.status.p, 4 * (size_t)B.n, cudaMemcpyDeviceToHost, E.stream));
 	CK(cudaStreamSynchronize(E.stream));
+	if (B.both) {
+		combine_strands(B.n_in, hd, hs, dist, status, strand);
+		return 0;
+	}
 	if (dist) memcpy(dist, hd, 4 * (size_t)B.n);
 	if (status) memcpy(status, hs, 4 * (size_t)B.n);
+	if (strand)
+		for (int32_t i = 0; i < B.n; ++i) strand[i] = hd[i] >= 0 ? 0 : -1;
 	return 0;
 }
 
@@ -744,13 +921,20 @@ static int prepare(const gwf_graph_t *g, const gwf_batch_opts_t *opt, GraphDev *
 		gwf_set_error("graph not indexed on a device: call gwf_ed_index first");
 		return GWF_E_NOT_INDEXED;
 	}
+	if (opt && opt->warps_per_read != 0 && opt->warps_per_read != 1 && opt->warps_per_read != 2 &&
+	    opt->warps_per_read != 4 && opt->warps_per_read != 8) {
+		gwf_set_error("warps_per_read must be 0, 1, 2, 4 or 8");
+		return GWF_E_BAD_INPUT;
+	}
 	int dev;
 	int rc = gwf_select_device((*G)->device, &dev);
 	if (rc) return rc;
-	(void)opt;
 	*E = gwf_engine(dev);
 	return *E ? 0 : GWF_E_CUDA;
 }
+
+// strand output of the gwf_ed_batch_concat call in progress on this thread (gwf_ed_batch_strand)
+static thread_local int32_t *t_strand_out = nullptr;
 
 extern "C" int gwf_ed_batch_concat(const gwf_graph_t *g, int32_t n, const char *seqs,
                                    const int64_t *offs, const int32_t *ql, const int32_t *v0,
@@ -773,16 +957,35 @@ extern "C" int gwf_ed_batch_concat(const gwf_graph_t *g, int32_t n, const char *
 	std::lock_guard<std::mutex> lk(g_batch_mu);
 	Batch *&B = g_scratch_batches[E->device];
 	if (!B) B = new Batch;
-	if ((rc = gwf_batch_load(*E, *B, n, seqs, offs, ql, v0, v1))) return rc;
-	const int32_t mode = opt ? opt->mode : GWF_MODE_AUTO;
 	const int32_t flags = opt ? opt->flags : 0;
+	if ((rc = gwf_batch_load(*E, *B, n, seqs, offs, ql, v0, v1, (flags & GWF_F_BOTH_STRANDS) != 0))) return rc;
+	const int32_t mode = opt ? opt->mode : GWF_MODE_AUTO;
 	const int32_t cps = opt ? opt->ctas_per_sm : 0;
 	const int32_t lag = (flags & GWF_F_MAX_LAG) ? (int32_t)std::min<uint32_t>(max_lag, INT32_MAX) : 0;
-	if ((rc = gwf_batch_exec(*E, *G, *B, mode, flags, cps, nullptr, nullptr, opt ? opt->use_graph : 0, lag)))
+	if ((rc = gwf_batch_exec(*E, *G, *B, mode, flags, cps, nullptr, nullptr, opt ? opt->use_graph : 0, lag,
+	                         opt ? opt->warps_per_read : 0)))
 		return rc;
 	std::vector<int32_t> st;
 	if (!status) st.resize((size_t)n), status = st.data();
-	return gwf_batch_fetch(*E, *B, dist, status);
+	return gwf_batch_fetch(*E, *B, dist, status, t_strand_out);
+}
+
+extern "C" int gwf_ed_batch_strand(const gwf_graph_t *g, int32_t n, const char *seqs, const int64_t *offs,
+                                   const int32_t *ql, const int32_t *v0, int32_t v1, uint32_t max_lag,
+                                   int32_t *dist, int32_t *status, int32_t *strand, const gwf_batch_opts_t *opt)
+{
+	if (n > 0 && !strand) {
+		gwf_set_error("gwf_ed_batch_strand: null strand array");
+		return GWF_E_BAD_INPUT;
+	}
+	gwf_batch_opts_t o;
+	if (opt) o = *opt;
+	else memset(&o, 0, sizeof o);
+	o.flags |= GWF_F_BOTH_STRANDS;
+	t_strand_out = strand;
+	const int rc = gwf_ed_batch_concat(g, n, seqs, offs, ql, v0, v1, max_lag, dist, status, &o);
+	t_strand_out = nullptr;
+	return rc;
 }
 
 extern "C" int gwf_ed_batch(const gwf_graph_t *g, int32_t n, const char *const *q, const int32_t *ql,
@@ -953,6 +1156,10 @@ extern "C" int gwf_ed_batch_align(const gwf_graph_t *g, int32_t n, const char *s
                                   int32_t *end_off, int32_t *path_n, int32_t *path_v, int32_t *path_arc,
                                   int32_t *cigar_n, uint32_t *cigar)
 {
+	if (flags & GWF_F_BOTH_STRANDS) {
+		gwf_set_error("traceback of both strands is not supported: align the reverse complement as its own read");
+		return GWF_E_UNSUPPORTED;
+	}
 	if (n < 0 || max_nv < 0 || max_ops < 0 ||
 	    (n > 0 && (!seqs || !offs || !ql || !v0 || !dist || !status || !end_off || !path_n ||
 	               (max_nv > 0 && (!path_v || !path_arc)) || (max_ops > 0 && (!cigar_n || !cigar))))) {
@@ -1052,7 +1259,8 @@ extern "C" gwf_batch_t *gwf_batch_create(const gwf_graph_t *g, int32_t n, const 
 	gwf_batch_s *b = new gwf_batch_s;
 	b->g = g;
 	std::lock_guard<std::mutex> lk(g_batch_mu);
-	if (gwf_batch_load(*E, b->B, n, seqs, offs, ql, v0, v1) || cudaStreamSynchronize(E->stream) != cudaSuccess) {
+	const bool both = opt && (opt->flags & GWF_F_BOTH_STRANDS);
+	if (gwf_batch_load(*E, b->B, n, seqs, offs, ql, v0, v1, both) || cudaStreamSynchronize(E->stream) != cudaSuccess) {
 		b->B.release();
 		delete b;
 		return nullptr;
@@ -1069,7 +1277,8 @@ extern "C" int gwf_batch_run(gwf_batch_t *b, const gwf_batch_opts_t *opt, float 
 	if (rc) return rc;
 	std::lock_guard<std::mutex> lk(g_batch_mu);
 	return gwf_batch_exec(*E, *G, b->B, opt ? opt->mode : GWF_MODE_AUTO, opt ? opt->flags : 0,
-	                      opt ? opt->ctas_per_sm : 0, kernel_ms, &b->launches, opt ? opt->use_graph : 0);
+	                      opt ? opt->ctas_per_sm : 0, kernel_ms, &b->launches, opt ? opt->use_graph : 0, 0,
+	                      opt ? opt->warps_per_read : 0);
 }
 
 extern "C" int gwf_batch_results(gwf_batch_t *b, int32_t *dist, int32_t *status)
@@ -1094,7 +1303,8 @@ extern "C" int gwf_batch_steps(gwf_batch_t *b, int32_t *steps)
 	if (rc) return rc;
 	std::lock_guard<std::mutex> lk(g_batch_mu);
 	if (b->B.n == 0) return 0;
-	CK(cudaMemcpyAsync(steps, b->B.steps.p, 4 * (size_t)b->B.n, cudaMemcpyDeviceToHost, E->stream));
+	// with both strands: the read's own strand (the first n_in entries)
+	CK(cudaMemcpyAsync(steps, b->B.steps.p, 4 * (size_t)b->B.n_in, cudaMemcpyDeviceToHost, E->stream));
 	CK(cudaStreamSynchronize(E->stream));
 	return 0;
 }

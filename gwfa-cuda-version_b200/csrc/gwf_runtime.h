@@ -37,6 +37,7 @@ struct Engine { // per-device launch state: stream, events, warp arenas
 	int device = 0;
 	int sm_count = 0;
 	int persistent_ctas_per_sm = 1;
+	int classes_ctas_per_sm = 1;
 	int64_t mem_budget = 0; // device bytes the arenas may take
 	cudaStream_t stream = nullptr;
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -49,14 +50,20 @@ struct Engine { // per-device launch state: stream, events, warp arenas
 
 struct Batch { // reads resident on the device
 	int32_t n = 0, v1 = -1, max_ql = 0;
+	int32_t n_in = 0;   // the caller's reads; n = 2 n_in with both strands (reverse complements after)
+	bool both = false;
 	int64_t pk_words = 0;
 	uint64_t generation = 0;          // bumped by every load (graph key)
 	int32_t dom_bucket = 0;           // length bucket with the largest sum of ql^2 (autotuner)
 	cudaGraphExec_t gexec = nullptr;  // captured level-0 sequence of the persistent form
-	uint64_t gkey[8] = {};
+	uint64_t gkey[9] = {};
 	std::vector<int32_t> h_ql;
 	HBuf h_meta; // pinned: raw offsets, packed offsets, queue order; results on the way back
 	DBuf raw, raw_off, ql, v0, pk, pk_off, pure, dist, status, steps, order_ql;
+	// read classes of the persistent form (reads aligned by groups of warps), cached per layout
+	DBuf order_cls;
+	uint64_t cls_key = ~0ULL;
+	int32_t cls_n = 0, cls_nw[4] = {}, cls_cnt[4] = {}, cls_cap[4] = {}, cls_start[4] = {};
 	void release();
 };
 
@@ -64,10 +71,11 @@ GraphDev *gwf_find_graph(const gwf_graph_t *g);
 Engine *gwf_engine(int dev);
 int gwf_select_device(int want, int *dev_out);
 int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64_t *offs,
-                   const int32_t *ql, const int32_t *v0, int32_t v1);
+                   const int32_t *ql, const int32_t *v0, int32_t v1, bool both = false);
 int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t flags,
-                   int ctas_per_sm, float *ms, int *launches_out, int use_graph = 0, int32_t max_lag = 0);
-int gwf_batch_fetch(Engine &E, Batch &B, int32_t *dist, int32_t *status);
+                   int ctas_per_sm, float *ms, int *launches_out, int use_graph = 0, int32_t max_lag = 0,
+                   int32_t warps_per_read = 0);
+int gwf_batch_fetch(Engine &E, Batch &B, int32_t *dist, int32_t *status, int32_t *strand = nullptr);
 namespace gwfb {
 struct KParams;
 struct SrvParams;
@@ -80,3 +88,5 @@ int gwf_serve_ctas_per_sm();
 std::mutex &gwf_batch_mutex();   // serialises batch calls (one engine per device)
 int gwf_tune_bucket(int32_t ql); // autotuner length bucket of a read
 int gwf_tune_lookup(int device, int32_t bucket, int32_t *form, int32_t *ctas_per_sm);
+int gwf_tune_lookup_nw(int device, int32_t bucket); // tuned warps per read, 0 = none
+extern const int32_t gwf_default_nw[]; // warps per read per length bucket when not tuned

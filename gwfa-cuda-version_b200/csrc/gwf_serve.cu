@@ -105,6 +105,7 @@ private:
 struct Request {
 	int64_t id = 0;
 	int32_t n = 0, v1 = -1;
+	int32_t n_in = 0; // the caller's reads; with both strands n = 2 n_in (reverse complements after)
 	std::vector<char> seqs;
 	std::vector<int64_t> offs;
 	std::vector<int32_t> ql, v0, dist, status;
@@ -528,9 +529,14 @@ extern "C" int64_t gwf_srv_submit(gwf_srv_t *S, int32_t n, const char *seqs, con
 		return GWF_E_BAD_INPUT;
 	}
 	auto r = std::make_shared<Request>();
-	r->n = n, r->v1 = v1;
+	const bool both = (S->flags & GWF_F_BOTH_STRANDS) != 0;
+	if (both && n > INT32_MAX / 2) {
+		gwf_set_error("gwf_srv_submit: too many reads");
+		return GWF_E_BAD_INPUT;
+	}
+	r->n_in = n, r->n = both ? 2 * n : n, r->v1 = v1;
 	int64_t tot = 0;
-	r->offs.resize((size_t)n);
+	r->offs.resize((size_t)r->n);
 	for (int32_t i = 0; i < n; ++i) {
 		if (ql[i] < 0) {
 			gwf_set_error("gwf_srv_submit: negative read length");
@@ -542,12 +548,22 @@ extern "C" int64_t gwf_srv_submit(gwf_srv_t *S, int32_t n, const char *seqs, con
 		}
 		r->offs[(size_t)i] = tot, tot += ql[i];
 	}
-	r->seqs.resize((size_t)tot + 16);
+	r->seqs.resize((size_t)(both ? 2 * tot : tot) + 16);
 	for (int32_t i = 0; i < n; ++i) memcpy(r->seqs.data() + r->offs[(size_t)i], seqs + offs[i], (size_t)ql[i]);
 	r->ql.assign(ql, ql + n);
 	r->v0.assign(v0, v0 + n);
-	r->dist.assign((size_t)n, -1);
-	r->status.assign((size_t)n, 0);
+	if (both) { // read n + i: the reverse complement of read i, from the same v0
+		for (int32_t i = 0; i < n; ++i) {
+			r->offs[(size_t)(n + i)] = tot + r->offs[(size_t)i];
+			const char *src = r->seqs.data() + r->offs[(size_t)i];
+			char *dst = r->seqs.data() + r->offs[(size_t)(n + i)];
+			for (int32_t j = 0; j < ql[i]; ++j) dst[ql[i] - 1 - j] = (char)gwf_comp_base((unsigned char)src[j]);
+		}
+		r->ql.insert(r->ql.end(), ql, ql + n);
+		r->v0.insert(r->v0.end(), v0, v0 + n);
+	}
+	r->dist.assign((size_t)r->n, -1);
+	r->status.assign((size_t)r->n, 0);
 	r->t_submit = now_s();
 	{
 		std::lock_guard<std::mutex> lk(S->mu);
@@ -564,10 +580,29 @@ extern "C" int64_t gwf_srv_submit(gwf_srv_t *S, int32_t n, const char *seqs, con
 	return r->id;
 }
 
-static int fill(const Request &r, int32_t *dist, int32_t *status)
+// Results of a finished request. With both strands, read i's two strands (i and n_in + i) give
+// the smaller distance (the read itself on a tie) and the strand; a strand with a non-OK status
+// makes the read's status that status and its distance -1 (as gwf_ed_batch_strand).
+static int fill(const Request &r, int32_t *dist, int32_t *status, int32_t *strand = nullptr)
 {
-	if (dist) memcpy(dist, r.dist.data(), sizeof(int32_t) * (size_t)r.n);
-	if (status) memcpy(status, r.status.data(), sizeof(int32_t) * (size_t)r.n);
+	if (r.n == r.n_in) {
+		if (dist) memcpy(dist, r.dist.data(), sizeof(int32_t) * (size_t)r.n);
+		if (status) memcpy(status, r.status.data(), sizeof(int32_t) * (size_t)r.n);
+		if (strand)
+			for (int32_t i = 0; i < r.n; ++i) strand[i] = r.dist[(size_t)i] >= 0 ? 0 : -1;
+		return 1;
+	}
+	for (int32_t i = 0; i < r.n_in; ++i) {
+		const int32_t df = r.dist[(size_t)i], dr = r.dist[(size_t)(r.n_in + i)];
+		const int32_t sf = r.status[(size_t)i], sr = r.status[(size_t)(r.n_in + i)];
+		int32_t d = -1, st = GWF_OK, k = -1;
+		if (sf != GWF_OK || sr != GWF_OK) st = sf != GWF_OK ? sf : sr;
+		else if (df >= 0 && (dr < 0 || df <= dr)) d = df, k = 0;
+		else if (dr >= 0) d = dr, k = 1;
+		if (dist) dist[i] = d;
+		if (status) status[i] = st;
+		if (strand) strand[i] = k;
+	}
 	return 1;
 }
 
@@ -591,6 +626,15 @@ extern "C" int gwf_srv_wait(gwf_srv_t *S, int64_t req, int32_t *dist, int32_t *s
 	if (!S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return r->done; }))
 		return GWF_E_TIMEOUT;
 	return fill(*r, dist, status);
+}
+
+extern "C" int gwf_srv_strand(gwf_srv_t *S, int64_t req, int32_t *strand)
+{
+	if (!S || !strand) return GWF_E_BAD_INPUT;
+	std::lock_guard<std::mutex> lk(S->mu);
+	auto it = S->all.find(req);
+	if (it == S->all.end() || !it->second->done) return GWF_E_BAD_INPUT;
+	return fill(*it->second, nullptr, nullptr, strand) == 1 ? 0 : GWF_E_BAD_INPUT;
 }
 
 extern "C" int gwf_srv_times(gwf_srv_t *S, int64_t req, double *t_submit, double *t_admit, double *t_done)

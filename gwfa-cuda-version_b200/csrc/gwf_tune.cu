@@ -2,11 +2,12 @@
 //
 // The cost of a read grows with ql^2 x error, and the arena a warp needs grows with ql, so the
 // best launch shape depends on the lengths in a batch. gwf_tune times, on the caller's own reads
-// and separately for each length bucket, the persistent form at every CTAs-per-SM count up to
-// the occupancy limit and the plain form, and keeps the fastest per bucket in a per-device
-// table. A batch run with mode GWF_MODE_AUTO and ctas_per_sm = 0 then uses the entry of the
-// bucket that carries most of its work (sum of ql^2). The table can be written to and read from
-// a small JSON file, so a tuned setting survives the process.
+// and separately for each length bucket, the persistent form with 1, 2, 4 and 8 warps per read at
+// every CTAs-per-SM count up to the occupancy limit, and the plain form, and keeps the fastest
+// per bucket in a per-device table. A batch run with mode GWF_MODE_AUTO then aligns each read
+// with the warps per read of its own bucket (one launch, read classes longest first) and takes
+// the form and CTAs per SM of the bucket that carries most of its work (sum of ql^2). The table
+// can be written to and read from a small JSON file, so a tuned setting survives the process.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,7 +28,7 @@ const int32_t kBucketMax[GWF_TUNE_NBUCKETS] = {1500, 3000, 6000, 12000, INT32_MA
 constexpr int kMaxDevices = 64;
 
 struct TuneEntry {
-	int32_t valid = 0, form = 0, cps = 0;
+	int32_t valid = 0, form = 0, cps = 0, nw = 1;
 	float rps = 0;
 };
 
@@ -56,6 +57,14 @@ int gwf_tune_bucket(int32_t ql)
 	return GWF_TUNE_NBUCKETS - 1;
 }
 
+int gwf_tune_lookup_nw(int device, int32_t bucket)
+{
+	if (device < 0 || device >= kMaxDevices || bucket < 0 || bucket >= GWF_TUNE_NBUCKETS) return 0;
+	std::lock_guard<std::mutex> lk(g_tune_mu);
+	const TuneEntry &e = g_tune[device][bucket];
+	return e.valid && e.form != GWF_MODE_PLAIN ? e.nw : 0;
+}
+
 int gwf_tune_lookup(int device, int32_t bucket, int32_t *form, int32_t *ctas_per_sm)
 {
 	if (device < 0 || device >= kMaxDevices || bucket < 0 || bucket >= GWF_TUNE_NBUCKETS) return 0;
@@ -82,9 +91,11 @@ static int write_json(const char *path, int device)
 	for (int b = 0; b < GWF_TUNE_NBUCKETS; ++b) {
 		const TuneEntry &e = g_tune[device][b];
 		if (!e.valid) continue;
-		fprintf(f, "%s\n  {\"bucket\": %d, \"ql_max\": %d, \"form\": \"%s\", \"ctas_per_sm\": %d, \"reads_per_s\": %.1f}",
+		fprintf(f,
+		        "%s\n  {\"bucket\": %d, \"ql_max\": %d, \"form\": \"%s\", \"ctas_per_sm\": %d, \"reads_per_s\": %.1f, "
+		        "\"warps_per_read\": %d}",
 		        first ? "" : ",", b, kBucketMax[b] == INT32_MAX ? -1 : kBucketMax[b], form_name(e.form), e.cps,
-		        (double)e.rps);
+		        (double)e.rps, e.nw);
 		first = false;
 	}
 	fprintf(f, "\n]}\n");
@@ -135,21 +146,28 @@ extern "C" int gwf_tune(const gwf_graph_t *g, int32_t n, const char *seqs, const
 			return rc;
 		}
 		TuneEntry best;
-		std::vector<std::pair<int32_t, int32_t>> cand;
-		for (int c = 1; c <= E->persistent_ctas_per_sm; ++c) cand.push_back({GWF_MODE_PERSISTENT, c});
-		cand.push_back({GWF_MODE_PLAIN, 0});
-		for (auto &fc : cand) {
+		struct Cand {
+			int32_t form, cps, nw;
+		};
+		std::vector<Cand> cand;
+		for (int nw : {1, 2, 4, 8}) {
+			const int occ = nw == 1 ? E->persistent_ctas_per_sm : E->classes_ctas_per_sm;
+			for (int c = 1; c <= occ; ++c) cand.push_back({GWF_MODE_PERSISTENT, c, nw});
+		}
+		cand.push_back({GWF_MODE_PLAIN, 0, 1});
+		for (const Cand &fc : cand) {
 			float best_ms = 0;
 			for (int rep = 0; rep < 3; ++rep) { // one warm-up, then the faster of two timed runs
 				float ms = 0;
-				if ((rc = gwf_batch_exec(*E, *G, B, fc.first, 0, fc.second, &ms, nullptr))) {
+				if ((rc = gwf_batch_exec(*E, *G, B, fc.form, 0, fc.cps, &ms, nullptr, 0, 0, fc.nw))) {
 					B.release();
 					return rc;
 				}
 				if (rep == 1 || (rep == 2 && ms < best_ms)) best_ms = ms;
 			}
 			const float rps = best_ms > 0 ? (float)k / (best_ms / 1000.0f) : 0.0f;
-			if (!best.valid || rps > best.rps) best.valid = 1, best.form = fc.first, best.cps = fc.second, best.rps = rps;
+			if (!best.valid || rps > best.rps)
+				best.valid = 1, best.form = fc.form, best.cps = fc.cps, best.nw = fc.nw, best.rps = rps;
 		}
 		B.release();
 		std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -195,6 +213,18 @@ extern "C" int gwf_tune_load(const char *json_path, int32_t device)
 		e.form = strcmp(form, "plain") == 0 ? GWF_MODE_PLAIN : GWF_MODE_PERSISTENT;
 		e.cps = e.form == GWF_MODE_PLAIN ? 0 : std::max(1, cps);
 		e.rps = (float)rps;
+		// warps per read (absent in tables written before the field existed: one warp)
+		e.nw = 1;
+		const size_t end = text.find('}', pos);
+		const size_t at = text.find("\"warps_per_read\":", pos);
+		if (at != std::string::npos && at < end) {
+			int nw = 1;
+			if (sscanf(text.c_str() + at, "\"warps_per_read\": %d", &nw) != 1 || (nw != 1 && nw != 2 && nw != 4 && nw != 8)) {
+				gwf_set_errorf("gwf_tune_load: bad warps_per_read in %s", json_path);
+				return GWF_E_BAD_INPUT;
+			}
+			e.nw = e.form == GWF_MODE_PLAIN ? 1 : nw;
+		}
 		++n_read;
 	}
 	if (n_read == 0) {
@@ -217,6 +247,18 @@ extern "C" int gwf_tune_get(int32_t device, int32_t bucket, int32_t *form, int32
 	if (ctas_per_sm) *ctas_per_sm = e.cps;
 	if (reads_per_s) *reads_per_s = e.rps;
 	return e.valid;
+}
+
+extern "C" int gwf_tune_get_shape(int32_t device, int32_t bucket, int32_t *form, int32_t *ctas_per_sm,
+                                  int32_t *warps_per_read, float *reads_per_s)
+{
+	const int rc = gwf_tune_get(device, bucket, form, ctas_per_sm, reads_per_s);
+	if (rc < 0) return rc;
+	if (warps_per_read) {
+		std::lock_guard<std::mutex> lk(g_tune_mu);
+		*warps_per_read = g_tune[device_or_current(device)][bucket].nw;
+	}
+	return rc;
 }
 
 extern "C" void gwf_tune_clear(int32_t device)

@@ -65,6 +65,14 @@ typedef struct {
                                    A heuristic: distances can only grow, or become -1 when no
                                    state is left. Off = max_lag ignored, as in the reference. */
 
+#define GWF_F_BOTH_STRANDS  0x4 /* align each read and its reverse complement (IUPAC complement,
+                                   made on the device) from the same v0 in one launch; the read's
+                                   distance is the smaller one (-1 when neither aligns).
+                                   gwf_ed_batch_strand also returns which strand gave it. No
+                                   reference counterpart: the reference aligns the read as given,
+                                   from v0's orientation only (main.cu:370, TODO at main.cu:404).
+                                   Honoured by the batch, resident-batch and serving calls. */
+
 /* execution forms */
 #define GWF_MODE_AUTO        0 /* persistent cost-ordered queue */
 #define GWF_MODE_PLAIN       1 /* one launch per batch, one warp per read */
@@ -74,7 +82,9 @@ typedef struct {
 	int32_t mode;        /* GWF_MODE_* */
 	int32_t flags;       /* GWF_F_* */
 	int32_t device;      /* CUDA device ordinal (-1 = current) */
-	int32_t warps_per_cta; /* must be 0: one warp aligns one read, 8 warps per CTA */
+	int32_t warps_per_read; /* persistent form: warps that align one read together (1, 2, 4 or 8;
+	                           0 = per read-length bucket, the gwf_tune value for GWF_MODE_AUTO,
+	                           else the library's default). The plain form uses one warp per read. */
 	int32_t ctas_per_sm;   /* persistent grid; 0 = the autotuned value for GWF_MODE_AUTO (see
 	                          gwf_tune), else the occupancy limit */
 	int32_t use_graph;     /* 1 = replay the persistent form's launch sequence as a CUDA graph */
@@ -114,6 +124,14 @@ int gwf_ed_batch(const gwf_graph_t *g, int32_t n, const char *const *q, const in
 int gwf_ed_batch_concat(const gwf_graph_t *g, int32_t n, const char *seqs, const int64_t *offs,
                         const int32_t *ql, const int32_t *v0, int32_t v1, uint32_t max_lag,
                         int32_t *dist, int32_t *status, const gwf_batch_opts_t *opt);
+
+/* gwf_ed_batch_concat with GWF_F_BOTH_STRANDS (implied), plus strand[i]: 0 when read i aligns
+ * best as given (ties included), 1 when its reverse complement does, -1 when neither aligns or
+ * the read has a non-OK status. A strand that ends with a per-read error (GWF_E_CAPACITY after
+ * the retries) makes status[i] that error and dist[i] = -1. */
+int gwf_ed_batch_strand(const gwf_graph_t *g, int32_t n, const char *seqs, const int64_t *offs,
+                        const int32_t *ql, const int32_t *v0, int32_t v1, uint32_t max_lag,
+                        int32_t *dist, int32_t *status, int32_t *strand, const gwf_batch_opts_t *opt);
 
 /* ---- traceback: the alignment path ----
  * The reference computes distances only: gwf_ed's traceback argument is unused there
@@ -192,19 +210,23 @@ int gwf_ed_batch_noalloc(const gwf_graph_t *g, int32_t n, int32_t max_ql, const 
                          void *stream);
 
 /* ---- autotuner (no reference counterpart) ----
- * Times the persistent form at 1..(occupancy limit) CTAs per SM and the plain form on the given
- * reads, separately for each read-length bucket (ql < 1500, < 3000, < 6000, < 12000, longer;
- * at most max_reads_per_bucket evenly spread reads each, 0 = 8192), and keeps the fastest shape
- * per bucket for the graph's device. Batch calls with mode GWF_MODE_AUTO and ctas_per_sm = 0
- * then use the entry of the bucket holding most of the batch's work (sum of ql^2). json_path !=
- * NULL also writes the table as JSON; gwf_tune_load reads it back (device -1 = current). The
- * kernel aligns each read with one warp, so warps per read is not a tuned dimension. */
+ * Times the persistent form with 1, 2, 4 and 8 warps per read at 1..(occupancy limit) CTAs per
+ * SM, and the plain form, on the given reads, separately for each read-length bucket (ql < 1500,
+ * < 3000, < 6000, < 12000, longer; at most max_reads_per_bucket evenly spread reads each, 0 =
+ * 8192), and keeps the fastest shape per bucket for the graph's device. Batch calls with mode
+ * GWF_MODE_AUTO then align each read with the warps per read of its own bucket (warps_per_read =
+ * 0), and take the form and CTAs per SM (ctas_per_sm = 0) of the bucket holding most of the
+ * batch's work (sum of ql^2). json_path != NULL also writes the table as JSON; gwf_tune_load
+ * reads it back (device -1 = current). */
 #define GWF_TUNE_NBUCKETS 5
 int gwf_tune(const gwf_graph_t *g, int32_t n, const char *seqs, const int64_t *offs, const int32_t *ql,
              const int32_t *v0, int32_t v1, int32_t max_reads_per_bucket, const char *json_path);
 int gwf_tune_load(const char *json_path, int32_t device);
 /* 1 = the bucket has an entry (form = GWF_MODE_*, ctas_per_sm, measured reads/s), 0 = none. */
 int gwf_tune_get(int32_t device, int32_t bucket, int32_t *form, int32_t *ctas_per_sm, float *reads_per_s);
+/* gwf_tune_get plus the bucket's warps per read. */
+int gwf_tune_get_shape(int32_t device, int32_t bucket, int32_t *form, int32_t *ctas_per_sm,
+                       int32_t *warps_per_read, float *reads_per_s);
 void gwf_tune_clear(int32_t device);
 
 /* Page-locked host memory for read buffers, so that batch copies run at full PCIe speed. */
@@ -235,6 +257,11 @@ int64_t gwf_srv_submit(gwf_srv_t *s, int32_t n, const char *seqs, const int64_t 
 int gwf_srv_poll(gwf_srv_t *s, int64_t req, int32_t *dist, int32_t *status);
 /* Waits at most timeout_s seconds. Returns 1 done, GWF_E_TIMEOUT, or another error. */
 int gwf_srv_wait(gwf_srv_t *s, int64_t req, int32_t *dist, int32_t *status, double timeout_s);
+/* With GWF_F_BOTH_STRANDS in the server's flags, every read of a request is aligned on both
+ * strands (its reverse complement is queued as a read of its own) and poll / wait return the
+ * better distance; this gives the strand of each read of a finished request (as
+ * gwf_ed_batch_strand). Returns 0 or a GWF_E_* code. */
+int gwf_srv_strand(gwf_srv_t *s, int64_t req, int32_t *strand);
 /* Submit, first-admission and completion times (seconds, steady clock) of a finished request. */
 int gwf_srv_times(gwf_srv_t *s, int64_t req, double *t_submit, double *t_admit, double *t_done);
 /* Counters of the server, in this order: kernel launches, reads re-queued in a larger arena,

@@ -97,3 +97,33 @@ def test_lag_option(G):
     assert np.array_equal(np.array(run("-l", "3", gfa, reads).stdout.split(), dtype=np.int64), base)
     pruned = np.array(run("-l", "3", "-P", gfa, reads).stdout.split(), dtype=np.int64)
     assert ((pruned >= base) | (pruned == -1)).all()
+
+
+@pytest.mark.gpu
+def test_both_strands_option(tmp_path):
+    """-b: the reads as given align on strand + with the plain distances; their reverse
+    complements align on strand - at the same distances."""
+    gfa = os.path.join(GOLD, "graph_1000.gfa")
+    reads = os.path.join(GOLD, "reads_200.fa")
+    plain = run(gfa, reads).stdout.split()
+    rows = [ln.split("\t") for ln in run("-b", gfa, reads).stdout.splitlines()]
+    assert all(s in "+-*" for _, s in rows)
+    assert all(int(d) <= int(p) for (d, _), p in zip(rows, plain))
+    comp = str.maketrans("ACGTacgt", "TGCAtgca")
+    rc = tmp_path / "rc.fa"
+    with open(rc, "w") as f:
+        seq = None
+        for line in open(reads).read().split("\n") + [">"]:
+            if line.startswith(">"):
+                if seq is not None:
+                    f.write(">r\n%s\n" % seq.translate(comp)[::-1])
+                seq = ""
+            else:
+                seq += line.strip()
+    rows_rc = [ln.split("\t") for ln in run("-b", gfa, str(rc)).stdout.splitlines()]
+    # the same two strands swapped: the same distances; a strand - becomes + (a tie stays +)
+    assert [d for d, _ in rows_rc] == [d for d, _ in rows]
+    for (_, s), (_, t) in zip(rows, rows_rc):
+        assert (s == "*") == (t == "*") and (s != "-" or t == "+")
+    assert sum(s == "+" for _, s in rows) > 0.9 * len(rows) and sum(t == "-" for _, t in rows_rc) > 0.8 * len(rows)
+    assert run("-b", "-t", gfa, reads, check=False).returncode == 1
