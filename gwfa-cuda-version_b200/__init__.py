@@ -62,7 +62,7 @@ class BatchOpts(ctypes.Structure):
 class SrvOpts(ctypes.Structure):
     _fields_ = [("arena_budget_bytes", ctypes.c_int64), ("max_inflight_reads", ctypes.c_int32),
                 ("flags", ctypes.c_int32), ("device", ctypes.c_int32), ("max_lag", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 6)]
+                ("warps_per_read", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
 
 
 class GwfReads(ctypes.Structure):
@@ -527,10 +527,10 @@ class ResidentBatch:
 class Server:
     """gwf_srv_*: continuous batching on a resident graph."""
 
-    def __init__(self, graph, arena_budget_bytes=0, max_inflight_reads=0, flags=0, max_lag=0):
+    def __init__(self, graph, arena_budget_bytes=0, max_inflight_reads=0, flags=0, max_lag=0, warps_per_read=0):
         self.graph = graph
         opt = SrvOpts(arena_budget_bytes=arena_budget_bytes, max_inflight_reads=max_inflight_reads, flags=flags,
-                      max_lag=max_lag)
+                      max_lag=max_lag, warps_per_read=warps_per_read)
         self.ptr = lib().gwf_srv_create(graph.ptr, ctypes.byref(opt))
         if not self.ptr:
             raise GwfError(GWF_E_CUDA, last_error())

@@ -22,7 +22,8 @@ struct GrpShm {              // per group, in shared memory
 	uint32_t red[2][8][4];   // per-warp min/max quadruples of the radix sort, double-buffered
 	uint32_t ctr[8];         // append counters (monotonic; positions are relative to a base)
 	int32_t claim;           // queue position claimed for the group
-	int32_t pad[7];
+	int32_t pad[5];
+	long long claim64;       // serving: queue position claimed for the group (-1 = leave)
 };
 enum { C_E = 0, C_N, C_F, C_BA, C_TA, C_KEYS };
 
@@ -925,6 +926,134 @@ __device__ __forceinline__ void run_class(const KParams &p, const ClassParams &c
 }
 
 #ifndef GWF_KERNELS_DECL_ONLY
+// Serving form with groups of NW warps: k_serve's claim, pack, align and completion steps, with
+// one read per group. The group's first thread claims (the same bounded, backed-off polling and
+// closing rule as k_serve, the leader group closing the kernel), the group packs the read and
+// aligns it with align_read_grp, and the first thread writes the completion record.
+template <int NW>
+__global__ void __launch_bounds__(256, 3) k_serve_grp(const __grid_constant__ SrvParams p)
+{
+	__shared__ GrpShm gsh[4];
+	if (threadIdx.x < 4 * 8) ((uint32_t *)gsh[threadIdx.x >> 3].ctr)[threadIdx.x & 7] = 0;
+	__syncthreads();
+	const int gi = (threadIdx.x >> 5) / NW;
+	Grp<NW> G;
+	G.init(gsh + gi, gi);
+	constexpr int GS = 32 * NW;
+	const bool leader = blockIdx.x == 0 && gi == 0;
+	for (int64_t guard = 0; guard < (1LL << 40); ++guard) {
+		if (G.rank == 0) {
+			long long h = -1;
+			const uint64_t t0 = globaltimer_ns();
+			uint32_t ns = 128;
+			for (int64_t spin = 0; spin < (1LL << 32); ++spin) {
+				if (ld_acquire_s32(p.stop)) break;
+				const unsigned long long head = *(volatile const unsigned long long *)p.q_head;
+				if (head & SRV_CLOSED) break;
+				const unsigned long long tail = ld_acquire_u64(p.q_tail);
+				if (head < tail) {
+					atomicAdd(p.busy, 1);
+					if (atomicCAS(p.q_head, head, head + 1) == head) {
+						h = (long long)head;
+						break;
+					}
+					atomicSub(p.busy, 1);
+					continue;
+				}
+				const int64_t idle = (int64_t)(globaltimer_ns() - t0);
+				if (idle > p.max_idle_ns ||
+				    (leader && idle > p.idle_ns && *(volatile const int32_t *)p.busy == 0)) {
+					atomicCAS(p.q_head, head, head | SRV_CLOSED);
+					continue;
+				}
+				__nanosleep(ns);
+				if (ns < 32768) ns *= 2;
+			}
+			gsh[gi].claim64 = h;
+		}
+		G.sync();
+		const long long h = *(volatile long long *)&gsh[gi].claim64;
+		G.sync(); // every thread has the claim before the next one is written
+		if (h < 0) break;
+		asm volatile("fence.acq_rel.gpu;" ::: "memory");
+		const SrvEntry *ep = p.q + (h & p.qmask);
+		const uint32_t seq = __ldcg((const unsigned int *)&ep->seq);
+		if (seq != (uint32_t)(h + 1)) {
+			if (G.rank == 0) {
+				atomicOr(p.err, SRV_ERR_SEQ);
+				atomicOr(p.q_head, SRV_CLOSED);
+				atomicSub(p.busy, 1);
+			}
+			break;
+		}
+		const int32_t tag = __ldcg(&ep->tag), ql = __ldcg(&ep->ql), v0 = __ldcg(&ep->v0);
+		const int32_t v1 = __ldcg(&ep->v1), level = __ldcg(&ep->level);
+		const long long aoff = __ldcg((const long long *)&ep->arena_off);
+		const long long abytes = __ldcg((const long long *)&ep->arena_bytes);
+		uint8_t *ab = p.arena + aoff;
+		SrvHdr *hdr = (SrvHdr *)ab;
+		uint64_t *pk = (uint64_t *)(ab + 256);
+		const uint8_t *raw = ab + 256 + srv_pk_bytes(ql);
+		const int32_t L = ql > 0 ? ql : 0;
+		const int32_t nwords = (L + 31) / 32 + 2;
+		bool ok = true;
+		for (int32_t w = G.rank; w < nwords; w += GS) {
+			uint64_t word = 0;
+			for (int32_t t = 0; t < 32; ++t) {
+				const int32_t i = w * 32 + t;
+				if (i < L) {
+					const uint8_t ch = (uint8_t)__ldcg((const unsigned char *)raw + i);
+					ok &= (ch == 'A' || ch == 'C' || ch == 'G' || ch == 'T');
+					word |= (uint64_t)((ch >> 1) & 3) << (2 * t);
+				}
+			}
+			pk[w] = word;
+		}
+		const bool pure = G.or_bits(ok ? 0u : 1u) == 0;
+		if (G.rank == 0) {
+			hdr->zero = 0, hdr->ql = ql, hdr->v0 = v0, hdr->pure = pure ? 1 : 0;
+			hdr->dist = -1, hdr->status = ST_CAPACITY;
+		}
+		G.sync();
+		int32_t dist = -1, st = ST_CAPACITY;
+		const int64_t qb = srv_qbytes(ql);
+		const Caps c = caps_for(ql, level, p.dens_milli);
+		if (qb + ws_layout(c).total <= abytes) {
+			KParams lp;
+			memset(&lp, 0, sizeof lp);
+			lp.g = p.g;
+			lp.r.pk = pk;
+			lp.r.pk_off = &hdr->zero;
+			lp.r.raw = raw;
+			lp.r.raw_off = &hdr->zero;
+			lp.r.ql = &hdr->ql;
+			lp.r.v0 = &hdr->v0;
+			lp.r.pure = &hdr->pure;
+			lp.r.v1 = v1;
+			lp.r.n = 1;
+			lp.dens_milli = p.dens_milli;
+			lp.flags = p.flags;
+			lp.max_lag = p.max_lag;
+			lp.dist = &hdr->dist;
+			lp.status = &hdr->status;
+			if (p.max_lag > 0) align_read_grp<NW, true>(lp, 0, ab + qb, ql, level, gsh + gi, gi);
+			else align_read_grp<NW, false>(lp, 0, ab + qb, ql, level, gsh + gi, gi);
+			G.sync();
+			dist = *(volatile int32_t *)&hdr->dist;
+			st = *(volatile int32_t *)&hdr->status;
+		}
+		if (G.rank == 0) {
+			const unsigned long long pos = atomicAdd(p.cq_tail, 1ULL);
+			volatile SrvDone *d = p.cq + (pos & p.cmask);
+			d->tag = tag, d->dist = dist, d->status = st;
+			__threadfence_system();
+			d->gen = (int32_t)((pos >> p.cq_shift) + 1);
+			atomicSub(p.busy, 1);
+		}
+		G.sync();
+	}
+}
+
 // Persistent form with read classes: the CTA's 8 warps run class 0's reads as groups of nw[0]
 // warps, then (after a CTA barrier) class 1's as groups of nw[1], and so on. The classes come
 // longest reads first, so the long reads start early and the short ones fill the tail.

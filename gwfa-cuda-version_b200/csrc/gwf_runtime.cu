@@ -889,16 +889,28 @@ cudaError_t gwf_launch_persistent(const KParams &p, int ctas, int threads, cudaS
 	return cudaGetLastError();
 }
 
-cudaError_t gwf_launch_serve(const SrvParams &p, int ctas, int threads, cudaStream_t s)
+cudaError_t gwf_launch_serve(const SrvParams &p, int ctas, int threads, cudaStream_t s, int warps_per_read)
 {
-	k_serve<<<ctas, threads, 0, s>>>(p);
+	switch (warps_per_read) {
+	case 2: k_serve_grp<2><<<ctas, threads, 0, s>>>(p); break;
+	case 4: k_serve_grp<4><<<ctas, threads, 0, s>>>(p); break;
+	case 8: k_serve_grp<8><<<ctas, threads, 0, s>>>(p); break;
+	default: k_serve<<<ctas, threads, 0, s>>>(p); break;
+	}
 	return cudaGetLastError();
 }
 
-int gwf_serve_ctas_per_sm()
+int gwf_serve_ctas_per_sm(int warps_per_read)
 {
 	int occ = 0;
-	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_serve, 256, 0) != cudaSuccess) {
+	cudaError_t e;
+	switch (warps_per_read) {
+	case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_serve_grp<2>, 256, 0); break;
+	case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_serve_grp<4>, 256, 0); break;
+	case 8: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_serve_grp<8>, 256, 0); break;
+	default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_serve, 256, 0); break;
+	}
+	if (e != cudaSuccess) {
 		cudaGetLastError();
 		return 1;
 	}

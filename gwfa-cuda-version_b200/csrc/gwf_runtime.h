@@ -81,8 +81,9 @@ struct KParams;
 struct SrvParams;
 }
 cudaError_t gwf_launch_persistent(const gwfb::KParams &p, int ctas, int threads, cudaStream_t s);
-cudaError_t gwf_launch_serve(const gwfb::SrvParams &p, int ctas, int threads, cudaStream_t s);
-int gwf_serve_ctas_per_sm();
+cudaError_t gwf_launch_serve(const gwfb::SrvParams &p, int ctas, int threads, cudaStream_t s,
+                             int warps_per_read = 1);
+int gwf_serve_ctas_per_sm(int warps_per_read = 1);
 
 #include <mutex>
 std::mutex &gwf_batch_mutex();   // serialises batch calls (one engine per device)

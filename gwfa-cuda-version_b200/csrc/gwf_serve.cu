@@ -126,7 +126,7 @@ struct gwf_srv_s {
 	const gwf_graph_t *g = nullptr;
 	GraphDev *G = nullptr;
 	int device = 0, sm_count = 0, ctas = 0;
-	int32_t flags = 0, max_lag = 0;
+	int32_t flags = 0, max_lag = 0, nw = 1; // nw: warps that align one read together
 	int64_t budget = 0;
 	uint32_t qcap = 0, ccap = 0;
 	int cq_shift = 0;
@@ -374,7 +374,7 @@ int launch(gwf_srv_s *S)
 	p.max_lag = S->max_lag;
 	p.idle_ns = kIdleNs;
 	p.max_idle_ns = kMaxIdleNs;
-	if (gwf_launch_serve(p, S->ctas, 256, S->kstream) != cudaSuccess) return -1;
+	if (gwf_launch_serve(p, S->ctas, 256, S->kstream, S->nw) != cudaSuccess) return -1;
 	if (cudaEventRecord(S->kdone, S->kstream) != cudaSuccess) return -1;
 	S->kernel_running = true;
 	++S->launches;
@@ -466,6 +466,12 @@ extern "C" gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t 
 	gwf_srv_s *S = new gwf_srv_s;
 	S->g = g, S->G = G, S->device = dev;
 	S->flags = opt ? opt->flags : 0;
+	S->nw = opt && opt->warps_per_read > 0 ? opt->warps_per_read : 1;
+	if (S->nw != 1 && S->nw != 2 && S->nw != 4 && S->nw != 8) {
+		gwf_set_error("gwf_srv_create: warps_per_read must be 0, 1, 2, 4 or 8");
+		delete S;
+		return nullptr;
+	}
 	S->max_lag = opt && (opt->flags & GWF_F_MAX_LAG) && opt->max_lag > 0 ? opt->max_lag : 0;
 	size_t fr = 0, tot = 0;
 	cudaMemGetInfo(&fr, &tot);
@@ -475,7 +481,7 @@ extern "C" gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t 
 	S->ccap = S->qcap;
 	while ((1u << S->cq_shift) < S->ccap) ++S->cq_shift;
 	cudaDeviceGetAttribute(&S->sm_count, cudaDevAttrMultiProcessorCount, dev);
-	S->ctas = S->sm_count * gwf_serve_ctas_per_sm();
+	S->ctas = S->sm_count * gwf_serve_ctas_per_sm(S->nw);
 	bool ok = cudaStreamCreateWithFlags(&S->kstream, cudaStreamNonBlocking) == cudaSuccess &&
 	          cudaStreamCreateWithFlags(&S->fstream, cudaStreamNonBlocking) == cudaSuccess &&
 	          cudaEventCreateWithFlags(&S->kdone, cudaEventDisableTiming) == cudaSuccess;

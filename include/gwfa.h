@@ -246,7 +246,9 @@ typedef struct {
 	int32_t flags;              /* GWF_F_* */
 	int32_t device;
 	int32_t max_lag;            /* with GWF_F_MAX_LAG in flags: the lag of the pruning */
-	int32_t reserved[6];
+	int32_t warps_per_read;     /* warps that align one read together: 1, 2, 4 or 8 (0 = 1); more
+	                               warps per read lower the latency of long reads */
+	int32_t reserved[5];
 } gwf_srv_opts_t;
 gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t *opt);
 /* Queues one request of n reads; returns a request id >= 0 or a GWF_E_* code. Copies the

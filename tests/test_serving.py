@@ -58,6 +58,27 @@ def test_mixed_requests_equal_solo_results(G):
     reqs = _requests(w, np.random.default_rng(5))
     served, stats = _serve_and_compare(G, g, w, reqs, [-1] * len(reqs))
     assert all((st == 0).all() for _, st in served)
+
+
+@pytest.mark.parametrize("nw", [2, 4, 8])
+def test_groups_of_warps_equal_solo_results(G, nw):
+    """warps_per_read > 1: each read is aligned by a group of warps of the resident kernel; the
+    results are those of the batch call, also with lag pruning and v1 targets."""
+    w = G.load_workload("config5", n=60)
+    g = w["graph"]
+    g.index()
+    reqs = _requests(w, np.random.default_rng(nw), max_reads=12)
+    served, stats = _serve_and_compare(G, g, w, reqs, [-1] * len(reqs), arena_budget_bytes=8 << 30,
+                                       warps_per_read=nw)
+    assert all((st == 0).all() for _, st in served)
+    w3 = G.load_workload("config3", n=120)
+    g3 = w3["graph"]
+    g3.index()
+    reqs3 = _requests(w3, np.random.default_rng(nw + 1), max_reads=20)
+    v1s = [-1 if i % 2 else 7 for i in range(len(reqs3))]
+    _serve_and_compare(G, g3, w3, reqs3, v1s, warps_per_read=nw)
+    with pytest.raises(G.GwfError):
+        G.Server(g3, warps_per_read=3)
     assert stats["launches"] >= 1 and stats["arena_used"] == 0
 
 
