@@ -2,12 +2,15 @@
 of gwf-ed.cu) and the reference's own CUDA outputs, bit for bit. All calls go through the C ABI
 of libgwfa_b200.so."""
 import os
+import sys
 
 import numpy as np
 import pytest
 
 from conftest import GOLD, read_fasta, read_golden
 from randgraph import cases
+
+sys.path.insert(0, GOLD)
 
 pytestmark = pytest.mark.gpu
 
@@ -92,6 +95,41 @@ def test_random_graphs_with_overlaps(G, O, overlap, exact):
         checked += 1
         g.close()
     assert checked > 200
+
+
+def _overlap_set(G, kind, n=300):
+    """The overlap golden sets of tests/golden/make_golden.py: GFA links "L a + b + nM"."""
+    from overlap_graph import overlap_gfa, overlap_reads
+    text, seqs, links = overlap_gfa(5 if kind == "uniform" else 7, mode=kind)
+    g = G.Graph.from_gfa_text(text)
+    seg2v = g.vertex_of_segment()
+    reads, starts = overlap_reads(6 if kind == "uniform" else 8, seqs, links, n)
+    cat, offs, lens = G.pack_reads(reads)
+    return g, (cat, offs, lens), np.array([seg2v[v] for v in starts], dtype=np.int32)
+
+
+@pytest.mark.parametrize("kind", ["uniform", "mixed"])
+def test_overlap_links_match_reference(G, O, kind):
+    """GFA links with overlaps, through the loader: with one overlap per target segment the
+    kernels equal the reference's own CUDA routine (golden) and its restatement, in both forms
+    and with groups of warps; with mixed overlaps they equal the entry-keyed rule, never above
+    the reference, whose own results equal the restatement of its queue order."""
+    idx, ref = read_golden("ref_overlap_%s.txt" % kind)
+    g, reads, v0 = _overlap_set(G, kind)
+    _indexed(G, g)
+    og = O.OracleGraph.from_graph(g)
+    cat, offs, lens = reads
+    fifo, _, _ = og.ed_batch(cat, offs, lens, v0, stats=False)
+    entry, _, _ = og.ed_batch(cat, offs, lens, v0, stats=False, entry_key=True)
+    sel = np.array(idx)
+    assert list(fifo[sel]) == ref  # the restatement of the reference, pinned by the reference
+    for mode, nw in ((G.MODE_PLAIN, 0), (G.MODE_PERSISTENT, 1), (G.MODE_PERSISTENT, 4)):
+        d, st = g.ed_batch(reads, v0, mode=mode, warps_per_read=nw)
+        assert (st == 0).all() and np.array_equal(d, entry)
+        if kind == "uniform":
+            assert list(d[sel]) == ref
+        else:
+            assert (d[sel] <= np.array(ref)).all()
 
 
 def test_lag_pruning_random_graphs_with_overlaps(G, O):

@@ -50,6 +50,31 @@ def test_oracle_mixed_overlaps_entry_key_is_exact(O):
     assert n_worse > 0  # the inputs do reach the order-dependent case
 
 
+@pytest.mark.parametrize("kind,seeds", [("uniform", (5, 6)), ("mixed", (7, 8))])
+def test_oracle_matches_reference_on_overlap_links(G, O, kind, seeds):
+    """GFA links with overlaps ("L a + b + nM", tests/golden/overlap_graph.py) through the
+    product loader: the restatement equals the reference's own CUDA routine on every read it was
+    given (tests/golden/ref_overlap_*.txt), also where the links into a segment differ."""
+    import sys
+    sys.path.insert(0, GOLD)
+    from overlap_graph import overlap_gfa, overlap_reads
+    idx, ref = read_golden("ref_overlap_%s.txt" % kind)
+    text, seqs, links = overlap_gfa(seeds[0], mode=kind)
+    g = G.Graph.from_gfa_text(text)
+    seg2v = g.vertex_of_segment()
+    reads, starts = overlap_reads(seeds[1], seqs, links, 300)
+    cat, offs, lens = G.pack_reads(reads)
+    v0 = np.array([seg2v[v] for v in starts], dtype=np.int32)
+    og = O.OracleGraph.from_graph(g)
+    d, _, _ = og.ed_batch(cat, offs, lens, v0, stats=False)
+    assert list(d[np.array(idx)]) == ref
+    e, _, _ = og.ed_batch(cat, offs, lens, v0, stats=False, entry_key=True)
+    assert (e <= d).all()
+    if kind == "uniform":
+        assert np.array_equal(e, d)
+    assert any(o > 0 for _, _, o in g.arcs())
+
+
 def test_oracle_quirk_adds_cost_on_short_start_vertex(O):
     """gwf-ed.cu:809,833: k=-1 against an unsigned max_k: a start vertex shorter than 32 bases
     does not extend at s=0, so a perfect match costs 1."""
