@@ -278,7 +278,7 @@ def run_serving(args):
     g = w["graph"]
     g.index()
     budget = int(args.serve_budget_gib * (1 << 30))
-    srv = G.Server(g, arena_budget_bytes=budget)
+    srv = G.Server(g, arena_budget_bytes=budget, warps_per_read=args.serve_warps)
     rng = np.random.default_rng(55)
     reqs = make_requests(w, rng)
     nreads = [len(r[1]) for r in reqs]
@@ -323,7 +323,8 @@ def run_serving(args):
         "higher_is_better": False, "dtype": "int32", "data": "synthetic",
         "config": {"workload": "config5: 5 Mbp graph resident; requests of U{1..256} reads, ql U[500,20000], "
                                "error U[1%,10%]; seeded Poisson arrivals", "reads": int(sum(nreads)),
-                   "requests": len(reqs), "arena_budget_gib": args.serve_budget_gib},
+                   "requests": len(reqs), "arena_budget_gib": args.serve_budget_gib,
+                   "warps_per_read": max(1, args.serve_warps)},
         "peak_reads_per_s": peak, "levels": levels, "server": stats,
         "plain_one_launch_per_request": plain,
         "plain_note": "plain capacity from measured per-request launches; latency by FIFO replay of the same "
@@ -432,6 +433,9 @@ def main():
     ap.add_argument("--serve-reads", type=int, default=6000)
     ap.add_argument("--serve-budget-gib", type=float, default=64.0)
     ap.add_argument("--plain-sample", type=int, default=6)
+    ap.add_argument("--warps-per-read", type=int, default=0,
+                    help="persistent form: 1, 2, 4 or 8 warps per read; 0 = per read by its share of the work")
+    ap.add_argument("--serve-warps", type=int, default=0, help="serving: warps per read (0 = 1)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.serving:
@@ -486,7 +490,7 @@ def main():
 
     use_graph = args.graph if mode == G.MODE_PERSISTENT else 0
     for _ in range(args.warmup):
-        batch.run(mode=mode, ctas_per_sm=args.ctas_per_sm, use_graph=use_graph)
+        batch.run(mode=mode, ctas_per_sm=args.ctas_per_sm, use_graph=use_graph, warps_per_read=args.warps_per_read)
     dist_gpu, status = batch.results()
     launches = 0
     times = []
@@ -496,7 +500,8 @@ def main():
         for _ in range(args.steps):
             flush.zero_()              # evict L2 between steps (256 MB > 126 MB L2)
             torch.cuda.synchronize()
-            times.append(batch.run(mode=mode, ctas_per_sm=args.ctas_per_sm, use_graph=use_graph))
+            times.append(batch.run(mode=mode, ctas_per_sm=args.ctas_per_sm, use_graph=use_graph,
+                                   warps_per_read=args.warps_per_read))
             launches += batch.launches()
         torch.cuda.synchronize()
     barrier()
@@ -527,7 +532,7 @@ def main():
         def e2e_call():
             if args.split:
                 return G.align_sharded(g, (w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode)[0]
-            g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode)
+            g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], mode=mode, warps_per_read=args.warps_per_read)
         for _ in range(2):
             e2e_call()
         barrier()
@@ -551,7 +556,7 @@ def main():
                    "l2": "flushed between steps (256 MB write)",
                    "parallelism": ("one batch split by cost over the ranks, distances all-gathered, graph replicated"
                                    if args.split else "reads sharded by rank, graph replicated")},
-        "form": args.mode, "cuda_graph": bool(use_graph),
+        "form": args.mode, "cuda_graph": bool(use_graph), "warps_per_read": args.warps_per_read or "by share of work",
         "gbases_per_s": job_bases / (ms / 1000.0) / 1e9,
         "e2e": ({"value": job_reads / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
                 if e2e_s else None),

@@ -630,31 +630,44 @@ static int enqueue_pack(Engine &E, Batch &B)
 
 // ---- read classes: reads aligned by groups of 2, 4 or 8 warps
 //
-// Each read gets a number of warps from its length bucket (the caller's forced value, the tuned
-// table, or gwf_default_nw). The reads of one count form a class; classes run longest reads
-// first (8, 4, 2, then 1 warp per read), each class's queue ordered longest read first. One
-// launch of k_align_classes runs all classes.
-const int32_t gwf_default_nw[GWF_TUNE_NBUCKETS] = {1, 1, 1, 1, 1};
+// Each read gets a number of warps: the caller's forced value, the tuned value of its length
+// bucket (GWF_MODE_AUTO), or by default its share of the batch's work. The default takes a read's
+// cost as ql^2 (the wavefront work grows with the length times the score, and the score with the
+// length) and the warp slots of the persistent grid as the workers: a read that costs more than
+// an even share of the batch per warp slot would finish after the rest, so it gets up to 8 warps,
+// as many as its cost is shares (rounded up to a power of two). A batch that fills the device with
+// reads of similar cost keeps one warp per read, the most efficient; a small batch or the longest
+// reads of a mixed one get groups, which finish each read sooner. The reads of one count form a
+// class; classes run longest reads first (8, 4, 2, then 1 warp per read), each class's queue
+// ordered longest read first. One launch of k_align_classes runs all classes.
 static const int32_t kClassNw[4] = {8, 4, 2, 1};
 
-// Class layout of the batch for the per-bucket warp counts nw_b; uploads the class queues when
-// the layout changed. Returns the number of classes with reads.
-static int plan_classes(Engine &E, Batch &B, const int32_t *nw_b)
+static int32_t share_nw(double cost, double share)
 {
-	uint64_t key = B.generation << 20;
+	if (!(cost > share)) return 1;
+	const double r = cost / share;
+	return r > 4 ? 8 : r > 2 ? 4 : 2;
+}
+
+// Class layout of the batch for the per-bucket warp counts nw_b (0 = by the read's share of the
+// batch's work over `slots` warp slots); uploads the class queues when the layout changed.
+static int plan_classes(Engine &E, Batch &B, const int32_t *nw_b, int64_t slots)
+{
+	uint64_t key = B.generation << 24 | (uint64_t)(slots & 0xfffff) << 20;
 	for (int b = 0; b < GWF_TUNE_NBUCKETS; ++b) key |= (uint64_t)(nw_b[b] & 15) << (4 * b);
 	if (key == B.cls_key) return 0;
-	int32_t cls_of_bucket[GWF_TUNE_NBUCKETS];
-	for (int b = 0; b < GWF_TUNE_NBUCKETS; ++b) {
-		cls_of_bucket[b] = 3;
-		for (int k = 0; k < 4; ++k)
-			if (kClassNw[k] == nw_b[b]) cls_of_bucket[b] = k;
-	}
+	double total = 0;
+	for (int32_t i = 0; i < B.n; ++i) total += (double)B.h_ql[(size_t)i] * (double)B.h_ql[(size_t)i];
+	const double share = total / (double)std::max<int64_t>(1, slots);
 	int32_t cnt[4] = {0, 0, 0, 0}, cap[4] = {0, 0, 0, 0};
 	std::vector<uint8_t> cls((size_t)B.n);
 	for (int32_t i = 0; i < B.n; ++i) {
 		const int32_t q = B.h_ql[(size_t)i];
-		const int k = cls_of_bucket[gwf_tune_bucket(q)];
+		int32_t nw = nw_b[gwf_tune_bucket(q)];
+		if (nw <= 0) nw = share_nw((double)q * (double)q, share);
+		int k = 3;
+		for (int j = 0; j < 4; ++j)
+			if (kClassNw[j] == nw) k = j;
 		cls[(size_t)i] = (uint8_t)k, ++cnt[k], cap[k] = std::max(cap[k], q);
 	}
 	// each class longest read first: counting sort over 64-base length buckets
@@ -668,10 +681,6 @@ static int plan_classes(Engine &E, Batch &B, const int32_t *nw_b)
 	for (size_t b = 0; b + 1 < c2.size(); ++b) c2[b + 1] += c2[b];
 	for (int32_t i = 0; i < B.n; ++i)
 		order[(size_t)c2[(size_t)(cls[(size_t)i] * nb + (nb - 1 - (B.h_ql[(size_t)i] >> 6)))]++] = i;
-	int rc;
-	if ((rc = B.order_cls.ensure(4 * (size_t)B.n + 4))) return rc;
-	CK(cudaMemcpyAsync(B.order_cls.p, order.data(), 4 * (size_t)B.n, cudaMemcpyHostToDevice, E.stream));
-	CK(cudaStreamSynchronize(E.stream)); // the host order vector goes out of scope
 	B.cls_n = 0;
 	for (int k = 0; k < 4; ++k)
 		if (cnt[k] > 0) {
@@ -679,6 +688,11 @@ static int plan_classes(Engine &E, Batch &B, const int32_t *nw_b)
 			B.cls_nw[j] = kClassNw[k], B.cls_cnt[j] = cnt[k], B.cls_cap[j] = cap[k], B.cls_start[j] = start[k];
 		}
 	B.cls_key = key;
+	if (B.cls_n == 1 && B.cls_nw[0] == 1) return 0; // one warp per read: the plain persistent queue
+	int rc;
+	if ((rc = B.order_cls.ensure(4 * (size_t)B.n + 4))) return rc;
+	CK(cudaMemcpyAsync(B.order_cls.p, order.data(), 4 * (size_t)B.n, cudaMemcpyHostToDevice, E.stream));
+	CK(cudaStreamSynchronize(E.stream)); // the host order vector goes out of scope
 	return 0;
 }
 
@@ -794,22 +808,23 @@ int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t
 	KParams p = base_params(E, G, B, flags);
 	p.max_lag = max_lag > 0 ? max_lag : 0;
 	// warps per read of each length bucket (persistent form): forced, tuned (GWF_MODE_AUTO), or
-	// the library's defaults
+	// 0: by the read's share of the batch's work (plan_classes)
 	int32_t nw_b[GWF_TUNE_NBUCKETS];
-	bool classes = false;
 	for (int b = 0; b < GWF_TUNE_NBUCKETS; ++b) {
 		int32_t nw = warps_per_read > 0 ? warps_per_read : 0;
 		if (!nw && mode == GWF_MODE_AUTO) nw = gwf_tune_lookup_nw(E.device, b);
-		if (!nw) nw = gwf_default_nw[b];
 		nw_b[b] = nw;
-		classes |= nw > 1;
 	}
 	if (mode == GWF_MODE_AUTO && ctas_per_sm <= 0) { // autotuned shape for the dominant length bucket
 		int32_t f = 0, c = 0;
 		if (gwf_tune_lookup(E.device, B.dom_bucket, &f, &c)) mode = f, ctas_per_sm = c;
 	}
-	classes = classes && mode != GWF_MODE_PLAIN;
-	if (classes && (rc = plan_classes(E, B, nw_b))) return rc;
+	bool classes = false;
+	if (mode != GWF_MODE_PLAIN) {
+		const int64_t slots = (int64_t)E.sm_count * E.persistent_ctas_per_sm * kWarpsPerCta;
+		if ((rc = plan_classes(E, B, nw_b, slots))) return rc;
+		classes = B.cls_n > 1 || B.cls_nw[0] > 1;
+	}
 	if (ctas_per_sm <= 0) ctas_per_sm = classes ? E.classes_ctas_per_sm : E.persistent_ctas_per_sm;
 	bool count_copied = false;
 	CK(cudaEventRecord(E.ev0, E.stream));

@@ -90,4 +90,3 @@ std::mutex &gwf_batch_mutex();   // serialises batch calls (one engine per devic
 int gwf_tune_bucket(int32_t ql); // autotuner length bucket of a read
 int gwf_tune_lookup(int device, int32_t bucket, int32_t *form, int32_t *ctas_per_sm);
 int gwf_tune_lookup_nw(int device, int32_t bucket); // tuned warps per read, 0 = none
-extern const int32_t gwf_default_nw[]; // warps per read per length bucket when not tuned

@@ -82,9 +82,12 @@ typedef struct {
 	int32_t mode;        /* GWF_MODE_* */
 	int32_t flags;       /* GWF_F_* */
 	int32_t device;      /* CUDA device ordinal (-1 = current) */
-	int32_t warps_per_read; /* persistent form: warps that align one read together (1, 2, 4 or 8;
-	                           0 = per read-length bucket, the gwf_tune value for GWF_MODE_AUTO,
-	                           else the library's default). The plain form uses one warp per read. */
+	int32_t warps_per_read; /* persistent form: warps that align one read together (1, 2, 4 or 8).
+	                           0 = per read: the gwf_tune value of its length bucket for
+	                           GWF_MODE_AUTO, else by its share of the batch's work (cost ql^2
+	                           against the persistent grid's warp slots): reads costing more than
+	                           one slot's even share get 2, 4 or 8 warps, the others one. The plain
+	                           form uses one warp per read. */
 	int32_t ctas_per_sm;   /* persistent grid; 0 = the autotuned value for GWF_MODE_AUTO (see
 	                          gwf_tune), else the occupancy limit */
 	int32_t use_graph;     /* 1 = replay the persistent form's launch sequence as a CUDA graph */
