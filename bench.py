@@ -324,7 +324,7 @@ def run_serving(args):
         "config": {"workload": "config5: 5 Mbp graph resident; requests of U{1..256} reads, ql U[500,20000], "
                                "error U[1%,10%]; seeded Poisson arrivals", "reads": int(sum(nreads)),
                    "requests": len(reqs), "arena_budget_gib": args.serve_budget_gib,
-                   "warps_per_read": max(1, args.serve_warps)},
+                   "warps_per_read": args.serve_warps or 8},
         "peak_reads_per_s": peak, "levels": levels, "server": stats,
         "plain_one_launch_per_request": plain,
         "plain_note": "plain capacity from measured per-request launches; latency by FIFO replay of the same "
@@ -435,7 +435,7 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=6)
     ap.add_argument("--warps-per-read", type=int, default=0,
                     help="persistent form: 1, 2, 4 or 8 warps per read; 0 = per read by its share of the work")
-    ap.add_argument("--serve-warps", type=int, default=0, help="serving: warps per read (0 = 1)")
+    ap.add_argument("--serve-warps", type=int, default=0, help="serving: warps per read (0 = the library default, 8)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.serving:

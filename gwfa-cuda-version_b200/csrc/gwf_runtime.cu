@@ -351,7 +351,7 @@ void Batch::release()
 {
 	for (DBuf *b : {&raw, &raw_off, &ql, &v0, &pk, &pk_off, &pure, &dist, &status, &steps, &order_ql, &order_cls})
 		b->release();
-	cls_key = ~0ULL;
+	cls_key = ~0ULL, cls_gen = ~0ULL;
 	h_meta.release();
 	if (gexec) cudaGraphExecDestroy(gexec), gexec = nullptr;
 }
@@ -635,7 +635,8 @@ static int enqueue_pack(Engine &E, Batch &B)
 // cost as ql^2 (the wavefront work grows with the length times the score, and the score with the
 // length) and the warp slots of the persistent grid as the workers: a read that costs more than
 // an even share of the batch per warp slot would finish after the rest, so it gets up to 8 warps,
-// as many as its cost is shares (rounded up to a power of two). A batch that fills the device with
+// as many as its cost is shares (rounded up to a power of two); a read whose arena would make the
+// live arenas too large gets more warps too (arena_nw). A batch that fills the device with
 // reads of similar cost keeps one warp per read, the most efficient; a small batch or the longest
 // reads of a mixed one get groups, which finish each read sooner. The reads of one count form a
 // class; classes run longest reads first (8, 4, 2, then 1 warp per read), each class's queue
@@ -649,13 +650,28 @@ static int32_t share_nw(double cost, double share)
 	return r > 4 ? 8 : r > 2 ? 4 : 2;
 }
 
+// Live arenas: the persistent kernel slows down sharply once the arenas of all its warp slots
+// together pass ~16 GiB (long reads on dense graphs, whose arrival sets are tens of MB per read,
+// accessed at random): 6,000 reads of 0.5-20 kbp on the 5 Mbp graph align at 1,368 reads/s with
+// one warp per read (120 GB of arenas, cut to the memory budget) and 3,161 with eight. A read
+// whose one-warp arenas over every slot would pass that gets enough warps per read to stay below.
+static const double kLiveArenaBytes = 16.0 * (1LL << 30);
+
+static int32_t arena_nw(int32_t ql, int32_t dens_milli, int64_t slots)
+{
+	const double bytes = (double)ws_layout(caps_for(ql, 0, dens_milli)).total * (double)slots;
+	return bytes <= kLiveArenaBytes ? 1 : bytes <= 2 * kLiveArenaBytes ? 2 : bytes <= 4 * kLiveArenaBytes ? 4 : 8;
+}
+
 // Class layout of the batch for the per-bucket warp counts nw_b (0 = by the read's share of the
 // batch's work over `slots` warp slots); uploads the class queues when the layout changed.
-static int plan_classes(Engine &E, Batch &B, const int32_t *nw_b, int64_t slots)
+static int plan_classes(Engine &E, Batch &B, const int32_t *nw_b, int64_t slots, int32_t dens_milli)
 {
-	uint64_t key = B.generation << 24 | (uint64_t)(slots & 0xfffff) << 20;
+	// the layout depends on the batch contents (generation), the warp slots, the graph density
+	// and the bucket counts
+	uint64_t key = (uint64_t)(uint32_t)slots << 20 | (uint64_t)(uint32_t)dens_milli << 40;
 	for (int b = 0; b < GWF_TUNE_NBUCKETS; ++b) key |= (uint64_t)(nw_b[b] & 15) << (4 * b);
-	if (key == B.cls_key) return 0;
+	if (key == B.cls_key && B.cls_gen == B.generation) return 0;
 	double total = 0;
 	for (int32_t i = 0; i < B.n; ++i) total += (double)B.h_ql[(size_t)i] * (double)B.h_ql[(size_t)i];
 	const double share = total / (double)std::max<int64_t>(1, slots);
@@ -664,7 +680,7 @@ static int plan_classes(Engine &E, Batch &B, const int32_t *nw_b, int64_t slots)
 	for (int32_t i = 0; i < B.n; ++i) {
 		const int32_t q = B.h_ql[(size_t)i];
 		int32_t nw = nw_b[gwf_tune_bucket(q)];
-		if (nw <= 0) nw = share_nw((double)q * (double)q, share);
+		if (nw <= 0) nw = std::max(share_nw((double)q * (double)q, share), arena_nw(q, dens_milli, slots));
 		int k = 3;
 		for (int j = 0; j < 4; ++j)
 			if (kClassNw[j] == nw) k = j;
@@ -687,7 +703,7 @@ static int plan_classes(Engine &E, Batch &B, const int32_t *nw_b, int64_t slots)
 			const int j = B.cls_n++;
 			B.cls_nw[j] = kClassNw[k], B.cls_cnt[j] = cnt[k], B.cls_cap[j] = cap[k], B.cls_start[j] = start[k];
 		}
-	B.cls_key = key;
+	B.cls_key = key, B.cls_gen = B.generation;
 	if (B.cls_n == 1 && B.cls_nw[0] == 1) return 0; // one warp per read: the plain persistent queue
 	int rc;
 	if ((rc = B.order_cls.ensure(4 * (size_t)B.n + 4))) return rc;
@@ -760,7 +776,7 @@ static int launch_level0_graph(Engine &E, Batch &B, const KParams &p, int ctas_p
 	                         (uint64_t)(uint32_t)p.flags | (uint64_t)(uint32_t)p.max_lag << 32,
 	                         (uint64_t)(uintptr_t)E.retry_n.p,
 	                         (uint64_t)(uintptr_t)E.h_small.p, (uint64_t)(uintptr_t)E.retry_list.p,
-	                         classes ? B.cls_key : ~0ULL};
+	                         classes ? B.cls_key ^ B.cls_gen << 40 : ~0ULL};
 	if (!B.gexec || memcmp(key, B.gkey, sizeof key) != 0) {
 		if (B.gexec) cudaGraphExecDestroy(B.gexec), B.gexec = nullptr;
 		CK(cudaStreamBeginCapture(E.stream, cudaStreamCaptureModeThreadLocal));
@@ -822,7 +838,7 @@ int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t
 	bool classes = false;
 	if (mode != GWF_MODE_PLAIN) {
 		const int64_t slots = (int64_t)E.sm_count * E.persistent_ctas_per_sm * kWarpsPerCta;
-		if ((rc = plan_classes(E, B, nw_b, slots))) return rc;
+		if ((rc = plan_classes(E, B, nw_b, slots, G.dens_milli))) return rc;
 		classes = B.cls_n > 1 || B.cls_nw[0] > 1;
 	}
 	if (ctas_per_sm <= 0) ctas_per_sm = classes ? E.classes_ctas_per_sm : E.persistent_ctas_per_sm;

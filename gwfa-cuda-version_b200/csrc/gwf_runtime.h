@@ -62,7 +62,7 @@ struct Batch { // reads resident on the device
 	DBuf raw, raw_off, ql, v0, pk, pk_off, pure, dist, status, steps, order_ql;
 	// read classes of the persistent form (reads aligned by groups of warps), cached per layout
 	DBuf order_cls;
-	uint64_t cls_key = ~0ULL;
+	uint64_t cls_key = ~0ULL, cls_gen = ~0ULL; // layout key and the batch generation it was made for
 	int32_t cls_n = 0, cls_nw[4] = {}, cls_cnt[4] = {}, cls_cap[4] = {}, cls_start[4] = {};
 	void release();
 };

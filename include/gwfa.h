@@ -85,9 +85,10 @@ typedef struct {
 	int32_t warps_per_read; /* persistent form: warps that align one read together (1, 2, 4 or 8).
 	                           0 = per read: the gwf_tune value of its length bucket for
 	                           GWF_MODE_AUTO, else by its share of the batch's work (cost ql^2
-	                           against the persistent grid's warp slots): reads costing more than
-	                           one slot's even share get 2, 4 or 8 warps, the others one. The plain
-	                           form uses one warp per read. */
+	                           against the persistent grid's warp slots) and by its arena size:
+	                           reads costing more than one slot's even share, or whose arenas over
+	                           every slot would pass 16 GiB, get 2, 4 or 8 warps, the others one.
+	                           The plain form uses one warp per read. */
 	int32_t ctas_per_sm;   /* persistent grid; 0 = the autotuned value for GWF_MODE_AUTO (see
 	                          gwf_tune), else the occupancy limit */
 	int32_t use_graph;     /* 1 = replay the persistent form's launch sequence as a CUDA graph */
@@ -249,8 +250,9 @@ typedef struct {
 	int32_t flags;              /* GWF_F_* */
 	int32_t device;
 	int32_t max_lag;            /* with GWF_F_MAX_LAG in flags: the lag of the pruning */
-	int32_t warps_per_read;     /* warps that align one read together: 1, 2, 4 or 8 (0 = 1); more
-	                               warps per read lower the latency of long reads */
+	int32_t warps_per_read;     /* warps that align one read together: 1, 2, 4 or 8; 0 = 8. More
+	                               warps per read lower the latency of each read; one warp per read
+	                               gives more throughput on short reads of sparse graphs */
 	int32_t reserved[5];
 } gwf_srv_opts_t;
 gwf_srv_t *gwf_srv_create(const gwf_graph_t *g, const gwf_srv_opts_t *opt);
