@@ -408,6 +408,57 @@ def run_features(args):
     print(json.dumps(out), flush=True)
 
 
+def run_case(args):
+    """Small fixed cases, one kernel each, sized for profiler captures (a few GB on the device):
+    config3-4k   k_align_persistent: 20,000 config-3 reads of at most 4 kbp, one warp per read,
+                 four launches;
+    classes      k_align_classes: 100 config-4 reads (10 kbp, 5 Mbp graph), warps per read by
+                 default (eight here), two batches;
+    cigar        k_cigar: 400 config-2 reads with paths and CIGARs, two batches;
+    serve        k_serve: four requests of ten config-5 reads on a one-warp server, 1 GiB budget."""
+    G = pkg()
+    c = args.case
+    if c == "config3-4k":
+        w = G.load_workload("config3", n=30000)
+        sel = np.nonzero(w["lens"] <= 4000)[0][:20000]
+        g = w["graph"]
+        g.index()
+        b = G.ResidentBatch(g, w["cat"], np.ascontiguousarray(w["offs"][sel]), np.ascontiguousarray(w["lens"][sel]),
+                            np.ascontiguousarray(w["v0"][sel]), mode=G.MODE_PERSISTENT)
+        ms = [b.run(warps_per_read=1, use_graph=0) for _ in range(4)]
+        _, st = b.results()
+        out = {"reads": len(sel), "bases": int(w["lens"][sel].sum()), "ms": ms}
+    elif c == "classes":
+        w = G.load_workload("config4", n=100)
+        g = w["graph"]
+        g.index()
+        for _ in range(2):
+            _, st = g.ed_batch((w["cat"], w["offs"], w["lens"]), w["v0"], mode=G.MODE_PERSISTENT)
+        out = {"reads": 100}
+    elif c == "cigar":
+        w = G.load_workload("config2", n=400)
+        g = w["graph"]
+        g.index()
+        for _ in range(2):
+            r = g.ed_path((w["cat"], w["offs"], w["lens"]), w["v0"], max_nv=64, as_arrays=True, max_ops=256)
+        st = r[1]
+        out = {"reads": 400, "cigars": int((r[6] > 0).sum())}
+    else:
+        w = G.load_workload("config5", n=40)
+        g = w["graph"]
+        g.index()
+        srv = G.Server(g, arena_budget_bytes=1 << 30, warps_per_read=1)
+        ids = [srv.submit((w["cat"], np.ascontiguousarray(w["offs"][a:a + 10]), np.ascontiguousarray(w["lens"][a:a + 10])),
+                          np.ascontiguousarray(w["v0"][a:a + 10])) for a in range(0, 40, 10)]
+        st = np.concatenate([srv.wait(rid, k, timeout_s=300)[1] for rid, k in ids])
+        srv.close()
+        out = {"reads": 40}
+    if not (np.asarray(st) == 0).all():
+        raise SystemExit("case %s: per-read errors" % c)
+    out["case"] = c
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -435,9 +486,14 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=6)
     ap.add_argument("--warps-per-read", type=int, default=0,
                     help="persistent form: 1, 2, 4 or 8 warps per read; 0 = per read by its share of the work")
+    ap.add_argument("--case", choices=["config3-4k", "classes", "cigar", "serve"],
+                    help="run one small fixed case of one kernel (profiler captures) instead")
     ap.add_argument("--serve-warps", type=int, default=0, help="serving: warps per read (0 = the library default, 8)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.case:
+        run_case(args)
+        return
     if args.serving:
         run_serving(args)
         return
