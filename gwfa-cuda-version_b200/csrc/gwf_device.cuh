@@ -471,64 +471,6 @@ static __device__ __noinline__ void warp_bitonic_sort_global(uint64_t *keys, int
 		}
 }
 
-// Sorts keys[0..n), 32 < n <= 32 * R, with optional int32 payload: R entries per lane in
-// registers (entry r * 32 + lane), a bitonic network whose exchanges are shuffles (distance < 32)
-// or swaps between a lane's own registers (distance 32 or 64). Unused entries hold PAD_KEY, which
-// sorts last. Equal keys are never exchanged, so no entry is lost or duplicated.
-template <int R>
-static __device__ __noinline__ void warp_sort_reg(uint64_t *keys, int32_t *vals, int32_t n)
-{
-	const int lane = threadIdx.x & 31;
-	__syncwarp();
-	uint64_t kr[R];
-	int32_t vr[R];
-#pragma unroll
-	for (int r = 0; r < R; ++r) {
-		const int32_t i = r * 32 + lane;
-		kr[r] = i < n ? keys[i] : PAD_KEY;
-		vr[r] = (vals && i < n) ? vals[i] : 0;
-	}
-#pragma unroll
-	for (int32_t k = 2; k <= 32 * R; k <<= 1)
-#pragma unroll
-		for (int32_t j = k >> 1; j > 0; j >>= 1) {
-			if (j >= 32) { // partners in the same lane: registers r and r ^ (j / 32)
-				const int rj = j >> 5;
-#pragma unroll
-				for (int r = 0; r < R; ++r)
-					if ((r & rj) == 0) {
-						const int32_t i = r * 32 + lane;
-						const bool up = (i & k) == 0;
-						const int q = r | rj;
-						if (up ? kr[q] < kr[r] : kr[q] > kr[r]) {
-							const uint64_t tk = kr[r];
-							const int32_t tv = vr[r];
-							kr[r] = kr[q], vr[r] = vr[q], kr[q] = tk, vr[q] = tv;
-						}
-					}
-				continue;
-			}
-#pragma unroll
-			for (int r = 0; r < R; ++r) {
-				const uint64_t other = __shfl_xor_sync(FULL, kr[r], j);
-				const int32_t ov = __shfl_xor_sync(FULL, vr[r], j);
-				const int32_t i = r * 32 + lane;
-				const bool up = (i & k) == 0, lower = (i & j) == 0;
-				if (lower == up ? other < kr[r] : other > kr[r]) kr[r] = other, vr[r] = ov;
-			}
-		}
-	__syncwarp();
-#pragma unroll
-	for (int r = 0; r < R; ++r) {
-		const int32_t i = r * 32 + lane;
-		if (i < n) {
-			keys[i] = kr[r];
-			if (vals) vals[i] = vr[r];
-		}
-	}
-	__syncwarp();
-}
-
 __device__ __forceinline__ void warp_bitonic_sort(uint64_t *keys, int32_t *vals, int32_t n)
 {
 	const int lane = threadIdx.x & 31;
@@ -549,14 +491,6 @@ __device__ __forceinline__ void warp_bitonic_sort(uint64_t *keys, int32_t *vals,
 			if (vals) vals[rank] = val;
 		}
 		__syncwarp();
-		return;
-	}
-	if (n <= 64) {
-		warp_sort_reg<2>(keys, vals, n);
-		return;
-	}
-	if (n <= 128) {
-		warp_sort_reg<4>(keys, vals, n);
 		return;
 	}
 	warp_bitonic_sort_global(keys, vals, n);
