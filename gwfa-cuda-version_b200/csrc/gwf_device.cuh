@@ -32,7 +32,6 @@ constexpr uint64_t PAD_KEY = ~0ULL;
 constexpr int32_t ST_OK = 0;
 constexpr int32_t ST_BAD_INPUT = -2;
 constexpr int32_t ST_CAPACITY = -4;
-constexpr int32_t ST_TIMEOUT = -8;
 
 struct DevGraph {
 	const uint32_t *len;     // [n_vtx]

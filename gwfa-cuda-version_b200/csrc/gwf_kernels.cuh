@@ -32,16 +32,6 @@ struct KParams {
 	int32_t *path_v;        // path vertices from v0
 	int32_t *path_arc;      // arc index into path_v[j] (-1 for j = 0)
 	int32_t max_nv;
-	// streamed upload (persistent form): the read bytes arrive in chunks of 1 << ready_shift bytes
-	// of the raw buffer while the kernel runs; ready[c] turns nonzero once chunk c (and every chunk
-	// before it) is on the device. Null: every byte is there. With pack set, each warp packs its
-	// read (pk_w, pure_w) before aligning it, in place of k_pack_reads.
-	const uint32_t *ready;
-	int32_t ready_shift;
-	int32_t pack;
-	uint64_t *pk_w;
-	uint8_t *pure_w;
-	int64_t ready_wait_ns; // bound of one read's wait for its chunk
 };
 
 // ---- serving: one resident kernel, warps pull single reads from a device queue
@@ -876,58 +866,6 @@ __global__ void __launch_bounds__(256, 2) k_align_trace(const __grid_constant__ 
 // Persistent form: each warp owns one arena (sized for ql_cap) and pulls reads from the
 // cost-ordered queue; each read uses the capacities of its own length, so a short read clears
 // and touches only the arena it needs.
-__device__ __forceinline__ uint64_t globaltimer_ns();
-__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p);
-
-// Streamed upload: waits (lane 0, backed-off polling bounded by p.ready_wait_ns) until the chunk
-// holding the read's last byte and the 16 bytes after it is on the device; chunks arrive in
-// order and are 128-byte aligned, so no cache line of a chunk is touched before its flag is set.
-// Then packs the read as k_pack_reads does, reading the bytes through L2 (they came by DMA while
-// the kernel ran). Returns false when the wait gave up.
-__device__ __noinline__ bool stream_read_in(const KParams &p, int32_t r)
-{
-	const int lane = threadIdx.x & 31;
-	const int32_t L = p.r.ql[r] > 0 ? p.r.ql[r] : 0;
-	bool ok = true;
-	if (lane == 0) {
-		const uint32_t c = (uint32_t)((p.r.raw_off[r] + L + 15) >> p.ready_shift);
-		const uint64_t t0 = globaltimer_ns();
-		uint32_t ns = 64;
-		for (int64_t spin = 0; ld_acquire_u32(p.ready + c) == 0; ++spin) {
-			if (spin > (1LL << 31) || (int64_t)(globaltimer_ns() - t0) > p.ready_wait_ns) {
-				ok = false;
-				break;
-			}
-			__nanosleep(ns);
-			if (ns < 4096) ns *= 2;
-		}
-	}
-	ok = __shfl_sync(FULL, ok, 0);
-	if (!ok) return false;
-	if (p.pack) {
-		const uint8_t *q = p.r.raw + p.r.raw_off[r];
-		const int32_t nw = (L + 31) / 32 + 2;
-		uint64_t *out = p.pk_w + p.r.pk_off[r];
-		bool pure = true;
-		for (int32_t w = lane; w < nw; w += 32) {
-			uint64_t word = 0;
-			for (int32_t t = 0; t < 32; ++t) {
-				const int32_t i = w * 32 + t;
-				if (i < L) {
-					const uint8_t ch = (uint8_t)__ldcg((const unsigned char *)q + i);
-					pure &= (ch == 'A' || ch == 'C' || ch == 'G' || ch == 'T');
-					word |= (uint64_t)((ch >> 1) & 3) << (2 * t);
-				}
-			}
-			out[w] = word;
-		}
-		pure = __all_sync(FULL, pure);
-		if (lane == 0) p.pure_w[r] = pure ? 1 : 0;
-		__syncwarp();
-	}
-	return true;
-}
-
 __global__ void __launch_bounds__(256, 3) k_align_persistent(const __grid_constant__ KParams p)
 {
 	const int lane = threadIdx.x & 31;
@@ -939,10 +877,6 @@ __global__ void __launch_bounds__(256, 3) k_align_persistent(const __grid_consta
 		qi = __shfl_sync(FULL, qi, 0);
 		if (qi >= p.n_order) break;
 		const int32_t r = p.order[qi];
-		if (p.ready && !stream_read_in(p, r)) {
-			if (lane == 0) p.dist[r] = -1, p.status[r] = ST_TIMEOUT;
-			continue;
-		}
 		align_read(p, r, wsb, p.ql_cap, p.level);
 	}
 }
@@ -957,12 +891,6 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 {
 	unsigned long long v;
 	asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-	return v;
-}
-__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p)
-{
-	uint32_t v;
-	asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
 	return v;
 }
 __device__ __forceinline__ int32_t ld_acquire_s32(const int32_t *p)

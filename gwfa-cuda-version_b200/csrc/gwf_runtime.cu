@@ -305,10 +305,6 @@ Engine::~Engine()
 	for (HBuf *b : {&h_small, &h_stage}) b->release();
 	for (cudaEvent_t e : stage_ev)
 		if (e) cudaEventDestroy(e);
-	ready.release();
-	h_ones.release();
-	if (ev_z) cudaEventDestroy(ev_z);
-	if (cstream) cudaStreamDestroy(cstream);
 	if (stream) cudaStreamDestroy(stream);
 	if (ev0) cudaEventDestroy(ev0);
 	if (ev1) cudaEventDestroy(ev1);
@@ -328,9 +324,7 @@ Engine *gwf_engine(int dev)
 	if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess ||
 	    cudaEventCreate(&E->ev0) != cudaSuccess || cudaEventCreate(&E->ev1) != cudaSuccess ||
 	    cudaEventCreateWithFlags(&E->stage_ev[0], cudaEventDisableTiming) != cudaSuccess ||
-	    cudaEventCreateWithFlags(&E->stage_ev[1], cudaEventDisableTiming) != cudaSuccess ||
-	    cudaStreamCreateWithFlags(&E->cstream, cudaStreamNonBlocking) != cudaSuccess ||
-	    cudaEventCreateWithFlags(&E->ev_z, cudaEventDisableTiming) != cudaSuccess) {
+	    cudaEventCreateWithFlags(&E->stage_ev[1], cudaEventDisableTiming) != cudaSuccess) {
 		cudaGetLastError();
 		gwf_set_error("stream/event creation failed");
 		delete E;
@@ -393,9 +387,8 @@ static int upload(Engine &E, void *dst, const void *src, size_t n)
 }
 
 int gwf_batch_load(Engine &E, Batch &B, int32_t n_in, const char *seqs, const int64_t *offs,
-                   const int32_t *ql_in, const int32_t *v0, int32_t v1, bool both, bool defer_raw)
+                   const int32_t *ql_in, const int32_t *v0, int32_t v1, bool both)
 {
-	defer_raw = defer_raw && !both; // the reverse complements are made from the uploaded reads
 	// with both strands the batch holds 2 n reads: read n + i is the reverse complement of read
 	// i, made on the device, with the same v0
 	const int32_t n = both ? 2 * n_in : n_in;
@@ -451,14 +444,9 @@ int gwf_batch_load(Engine &E, Batch &B, int32_t n_in, const char *seqs, const in
 	    (rc = B.order_ql.ensure(4 * (size_t)n + 4)))
 		return rc;
 	cudaStream_t s = E.stream;
-	B.raw_pending = false;
 	if (n > 0) {
-		if (defer_raw) { // gwf_batch_exec uploads the bytes, streamed under the kernel if it can
-			B.h_raw_src = seqs + lo, B.raw_span = span, B.raw_pending = true;
-		} else {
-			if ((rc = upload(E, B.raw.p, seqs + lo, (size_t)span))) return rc;
-			CK(cudaMemsetAsync((char *)B.raw.p + span, 0, 16, s));
-		}
+		if ((rc = upload(E, B.raw.p, seqs + lo, (size_t)span))) return rc;
+		CK(cudaMemsetAsync((char *)B.raw.p + span, 0, 16, s));
 		CK(cudaMemcpyAsync(B.raw_off.p, h_raw_off, 8 * (size_t)n, cudaMemcpyHostToDevice, s));
 		if ((rc = upload(E, B.ql.p, ql_in, 4 * (size_t)n_in)) || (rc = upload(E, B.v0.p, v0, 4 * (size_t)n_in)))
 			return rc;
@@ -771,67 +759,6 @@ static int enqueue_classes(Engine &E, KParams p, const ClassLaunch &cl)
 	return 0;
 }
 
-// Streamed upload under the persistent kernel (gwf_ed_batch_concat, one warp per read). The read
-// bytes go up on the copy stream in chunks of 4 MiB (line-aligned), each followed by its flag;
-// the kernel is launched first, and each warp waits for the chunk holding its read, then packs
-// the read itself (no k_pack_reads). Reads in the queue's order need chunks in about upload order
-// when the lengths are alike (the order is stable within a length bucket), so alignment starts
-// after the first chunk instead of after the whole batch.
-static const int kStreamShift = 22;
-
-static int launch_streamed(Engine &E, const KParams &p, Batch &B, int ctas_per_sm, int *launches)
-{
-	const int64_t chunk = 1LL << kStreamShift, total = B.raw_span + 16;
-	const int64_t nch = (total + chunk - 1) >> kStreamShift;
-	int rc;
-	// pinned source of the flags (word 0 = 1) and of the zero padding (bytes 16..31); everything
-	// on the copy stream is a DMA copy, never a kernel, so it cannot wait behind the running
-	// persistent kernel for a free SM
-	if ((rc = E.ready.ensure(4 * (size_t)nch)) || (rc = E.h_ones.ensure(64))) return rc;
-	memset(E.h_ones.p, 0, 64);
-	*(volatile uint32_t *)E.h_ones.p = 1;
-	CK(cudaMemsetAsync(E.ready.p, 0, 4 * (size_t)nch, E.stream));
-	CK(cudaEventRecord(E.ev_z, E.stream));
-	CK(cudaStreamWaitEvent(E.cstream, E.ev_z, 0));
-	KParams q = p;
-	q.ready = (const uint32_t *)E.ready.p;
-	q.ready_shift = kStreamShift;
-	q.pack = 1;
-	q.pk_w = (uint64_t *)B.pk.p;
-	q.pure_w = (uint8_t *)B.pure.p;
-	q.ready_wait_ns = 60LL * 1000000000LL;
-	if ((rc = launch_persistent(E, q, (const int32_t *)B.order_ql.p, B.n, B.max_ql, 0, ctas_per_sm, launches)))
-		return rc;
-	// the copies, chunk by chunk, while the kernel runs; a pageable source passes through the two
-	// pinned staging chunks in turn
-	cudaPointerAttributes at;
-	const bool pinned =
-	    cudaPointerGetAttributes(&at, B.h_raw_src) == cudaSuccess && at.type == cudaMemoryTypeHost;
-	cudaGetLastError();
-	if (!pinned && (rc = E.h_stage.ensure(2 * (size_t)chunk))) return rc;
-	for (int64_t c = 0; c < nch; ++c) {
-		const int64_t off = c * chunk, len = std::min(chunk, B.raw_span - off);
-		if (len > 0) {
-			const char *src = B.h_raw_src + off;
-			if (!pinned) {
-				const int b = (int)(c & 1);
-				CK(cudaEventSynchronize(E.stage_ev[b])); // the copy that last read this staging chunk
-				char *stage = (char *)E.h_stage.p + b * chunk;
-				memcpy(stage, src, (size_t)len);
-				src = stage;
-			}
-			CK(cudaMemcpyAsync((char *)B.raw.p + off, src, (size_t)len, cudaMemcpyHostToDevice, E.cstream));
-			if (!pinned) CK(cudaEventRecord(E.stage_ev[(int)(c & 1)], E.cstream));
-		}
-		if (c == nch - 1)
-			CK(cudaMemcpyAsync((char *)B.raw.p + B.raw_span, (const char *)E.h_ones.p + 16, 16, cudaMemcpyHostToDevice,
-			                   E.cstream));
-		CK(cudaMemcpyAsync((uint32_t *)E.ready.p + c, E.h_ones.p, 4, cudaMemcpyHostToDevice, E.cstream));
-	}
-	B.raw_pending = false;
-	return 0;
-}
-
 // Level-0 sequence of the persistent form as one CUDA graph: pack, clear the overflow count,
 // persistent kernel, copy the overflow count to the host. Captured once per batch contents and
 // launch shape, replayed on every run.
@@ -915,19 +842,9 @@ int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t
 		classes = B.cls_n > 1 || B.cls_nw[0] > 1;
 	}
 	if (ctas_per_sm <= 0) ctas_per_sm = classes ? E.classes_ctas_per_sm : E.persistent_ctas_per_sm;
-	// deferred read bytes: streamed under the one-warp persistent kernel, else uploaded now
-	const bool streamed = B.raw_pending && mode != GWF_MODE_PLAIN && !classes && !use_graph;
-	if (B.raw_pending && !streamed) {
-		if ((rc = upload(E, B.raw.p, B.h_raw_src, (size_t)B.raw_span))) return rc;
-		CK(cudaMemsetAsync((char *)B.raw.p + B.raw_span, 0, 16, E.stream));
-		B.raw_pending = false;
-	}
 	bool count_copied = false;
 	CK(cudaEventRecord(E.ev0, E.stream));
-	if (streamed) {
-		CK(cudaMemsetAsync(E.retry_n.p, 0, 4, E.stream));
-		if ((rc = launch_streamed(E, p, B, ctas_per_sm, &launches))) return rc;
-	} else if (use_graph && mode != GWF_MODE_PLAIN) {
+	if (use_graph && mode != GWF_MODE_PLAIN) {
 		if ((rc = launch_level0_graph(E, B, p, ctas_per_sm, classes))) return rc;
 		launches += 2;
 		count_copied = true;
@@ -970,7 +887,6 @@ int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t
 	}
 	CK(cudaEventRecord(E.ev1, E.stream));
 	CK(cudaEventSynchronize(E.ev1));
-	CK(cudaStreamSynchronize(E.cstream)); // streamed copies: the caller's buffer is free on return
 	if (ms) CK(cudaEventElapsedTime(ms, E.ev0, E.ev1));
 	if (launches_out) *launches_out = launches;
 	return 0;
@@ -1085,7 +1001,7 @@ extern "C" int gwf_ed_batch_concat(const gwf_graph_t *g, int32_t n, const char *
 	Batch *&B = g_scratch_batches[E->device];
 	if (!B) B = new Batch;
 	const int32_t flags = opt ? opt->flags : 0;
-	if ((rc = gwf_batch_load(*E, *B, n, seqs, offs, ql, v0, v1, (flags & GWF_F_BOTH_STRANDS) != 0, true))) return rc;
+	if ((rc = gwf_batch_load(*E, *B, n, seqs, offs, ql, v0, v1, (flags & GWF_F_BOTH_STRANDS) != 0))) return rc;
 	const int32_t mode = opt ? opt->mode : GWF_MODE_AUTO;
 	const int32_t cps = opt ? opt->ctas_per_sm : 0;
 	const int32_t lag = (flags & GWF_F_MAX_LAG) ? (int32_t)std::min<uint32_t>(max_lag, INT32_MAX) : 0;

@@ -45,10 +45,6 @@ struct Engine { // per-device launch state: stream, events, warp arenas
 	HBuf h_small;
 	HBuf h_stage;                              // two pinned chunks for pageable uploads
 	cudaEvent_t stage_ev[2] = {nullptr, nullptr};
-	cudaStream_t cstream = nullptr;            // streamed uploads: the copy stream
-	cudaEvent_t ev_z = nullptr;                // streamed uploads: flags cleared
-	DBuf ready;                                // streamed uploads: one flag per chunk
-	HBuf h_ones;                               // pinned source of the flags
 	~Engine();
 };
 
@@ -56,11 +52,6 @@ struct Batch { // reads resident on the device
 	int32_t n = 0, v1 = -1, max_ql = 0;
 	int32_t n_in = 0;   // the caller's reads; n = 2 n_in with both strands (reverse complements after)
 	bool both = false;
-	// deferred read bytes (gwf_ed_batch_concat): uploaded by gwf_batch_exec, streamed under the
-	// persistent kernel when it can be
-	const char *h_raw_src = nullptr;
-	int64_t raw_span = 0;
-	bool raw_pending = false;
 	int64_t pk_words = 0;
 	uint64_t generation = 0;          // bumped by every load (graph key)
 	int32_t dom_bucket = 0;           // length bucket with the largest sum of ql^2 (autotuner)
@@ -80,8 +71,7 @@ GraphDev *gwf_find_graph(const gwf_graph_t *g);
 Engine *gwf_engine(int dev);
 int gwf_select_device(int want, int *dev_out);
 int gwf_batch_load(Engine &E, Batch &B, int32_t n, const char *seqs, const int64_t *offs,
-                   const int32_t *ql, const int32_t *v0, int32_t v1, bool both = false,
-                   bool defer_raw = false);
+                   const int32_t *ql, const int32_t *v0, int32_t v1, bool both = false);
 int gwf_batch_exec(Engine &E, const GraphDev &G, Batch &B, int32_t mode, int32_t flags,
                    int ctas_per_sm, float *ms, int *launches_out, int use_graph = 0, int32_t max_lag = 0,
                    int32_t warps_per_read = 0);
