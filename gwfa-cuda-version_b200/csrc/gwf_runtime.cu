@@ -663,6 +663,22 @@ static int32_t arena_nw(int32_t ql, int32_t dens_milli, int64_t slots)
 	return bytes <= kLiveArenaBytes ? 1 : bytes <= 2 * kLiveArenaBytes ? 2 : bytes <= 4 * kLiveArenaBytes ? 4 : 8;
 }
 
+// The shortest read lengths (up to max_ql + 1) from which arena_nw gives 2, 4 and 8 warps: the
+// arena grows with the length, so a binary search per level replaces a layout per read.
+static void arena_nw_lengths(int32_t max_ql, int32_t dens_milli, int64_t slots, int32_t from[3])
+{
+	for (int lv = 0; lv < 3; ++lv) {
+		const int32_t want = 2 << lv;
+		int32_t lo = 1, hi = max_ql + 1; // first length in [lo, hi] with arena_nw >= want
+		while (lo < hi) {
+			const int32_t mid = lo + (hi - lo) / 2;
+			if (arena_nw(mid, dens_milli, slots) >= want) hi = mid;
+			else lo = mid + 1;
+		}
+		from[lv] = lo;
+	}
+}
+
 // Class layout of the batch for the per-bucket warp counts nw_b (0 = by the read's share of the
 // batch's work over `slots` warp slots); uploads the class queues when the layout changed.
 static int plan_classes(Engine &E, Batch &B, const int32_t *nw_b, int64_t slots, int32_t dens_milli)
@@ -675,12 +691,15 @@ static int plan_classes(Engine &E, Batch &B, const int32_t *nw_b, int64_t slots,
 	double total = 0;
 	for (int32_t i = 0; i < B.n; ++i) total += (double)B.h_ql[(size_t)i] * (double)B.h_ql[(size_t)i];
 	const double share = total / (double)std::max<int64_t>(1, slots);
+	int32_t from[3];
+	arena_nw_lengths(B.max_ql, dens_milli, slots, from);
 	int32_t cnt[4] = {0, 0, 0, 0}, cap[4] = {0, 0, 0, 0};
 	std::vector<uint8_t> cls((size_t)B.n);
 	for (int32_t i = 0; i < B.n; ++i) {
 		const int32_t q = B.h_ql[(size_t)i];
 		int32_t nw = nw_b[gwf_tune_bucket(q)];
-		if (nw <= 0) nw = std::max(share_nw((double)q * (double)q, share), arena_nw(q, dens_milli, slots));
+		if (nw <= 0)
+			nw = std::max(share_nw((double)q * (double)q, share), q >= from[2] ? 8 : q >= from[1] ? 4 : q >= from[0] ? 2 : 1);
 		int k = 3;
 		for (int j = 0; j < 4; ++j)
 			if (kClassNw[j] == nw) k = j;
