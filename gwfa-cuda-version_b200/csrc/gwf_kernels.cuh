@@ -224,22 +224,32 @@ __device__ __noinline__ void align_read_t(const KParams &p, int32_t r, uint8_t *
 		bool found = false, ovf = false;
 		int32_t f_j = 0x7fffffff, f_t = -1, f_k = -1; // TR: this lane's first end state
 
-		// ---- phase 1: extend every diagonal; collect vertex-end (and, for v1 >= 0,
-		// query-end) states into the first wave (gwf-ed.cu:902-910, 965-984)
-		int32_t n_e = 0;
-		for (int32_t base = 0; base < n_a; base += 32) {
+		// ---- phases 1 and 2, in one pass over the wavefront. Phase 1 extends every diagonal and
+		// collects the vertex-end (and, for v1 >= 0, query-end) states into the first wave
+		// (gwf-ed.cu:902-910, 965-984). Phase 2 forms the in-vertex successors, sorted and unique by
+		// construction (gwf_ed_extend_batch, gwf-ed.cu:912-1016). Phase 2 runs one diagonal behind
+		// phase 1, so that both neighbours of a diagonal are extended when its successors are
+		// formed: in the chunk at `base`, lane l extends diagonal base+l and forms the successors of
+		// diagonal base+l-1. The diagonal and its left neighbour come by rotating shuffles; lanes 30
+		// and 31 hand over their diagonals of the previous chunk (o_*), which are the left
+		// neighbours of the chunk's first two.
+		int32_t n_e = 0, n_x = 0, n_tb = 0;
+		uint64_t o_vd = 0;
+		int32_t o_k = 0, o_t = 0, o_vl = 0;
+		const int src1 = (lane + 31) & 31, src2 = (lane + 30) & 31;
+		for (int32_t base = 0; base <= n_a; base += 32) {
 			const int32_t j = base + lane;
 			bool toE = false;
 			uint64_t vd = 0;
-			int32_t k = 0, t = 0;
+			int32_t k = 0, t = 0, vl = 0;
 			if (j < n_a) {
 				vd = A_VD[j];
 				k = A_K[j];
 				if constexpr (TR) t = A_T[j];
 				const uint32_t v = vd_v(vd);
-				const int32_t d = vd_d(vd), vl = (int32_t)__ldg(g.len + v);
+				const int32_t d = vd_d(vd);
+				vl = (int32_t)__ldg(g.len + v);
 				k = ext(g, rc, v, d, k, vl);
-				A_K[j] = k;
 				const bool vend = k == vl - 1, qend = d + k == ql - 1;
 				if (qend) {
 					if (v1 < 0 || ((int32_t)v == v1 && vend)) {
@@ -250,13 +260,92 @@ __device__ __noinline__ void align_read_t(const KParams &p, int32_t r, uint8_t *
 				} else if (vend)
 					toE = true;
 			}
-			const uint32_t m = __ballot_sync(FULL, toE);
-			const int32_t pos = n_e + __popc(m & lanemask_lt());
-			if (toE && pos < c.w) {
-				E_VD[pos] = vd, E_K[pos] = k;
-				if constexpr (TR) E_T[pos] = t;
+			{
+				const uint32_t m = __ballot_sync(FULL, toE);
+				const int32_t pos = n_e + __popc(m & lanemask_lt());
+				if (toE && pos < c.w) {
+					E_VD[pos] = vd, E_K[pos] = k;
+					if constexpr (TR) E_T[pos] = t;
+				}
+				n_e += __popc(m);
 			}
-			n_e += __popc(m);
+
+			// diagonal e = j - 1 (mine) and e - 1 (left); e + 1 (right) is this lane's own
+			const bool h1 = lane == 31, h2 = lane >= 30;
+			const uint64_t my_vd = __shfl_sync(FULL, h1 ? o_vd : vd, src1);
+			const int32_t my_k = __shfl_sync(FULL, h1 ? o_k : k, src1);
+			const int32_t my_vl = __shfl_sync(FULL, h1 ? o_vl : vl, src1);
+			const uint64_t pv = __shfl_sync(FULL, h2 ? o_vd : vd, src2);
+			const int32_t pk = __shfl_sync(FULL, h2 ? o_k : k, src2);
+			int32_t tt = 0, pt = 0;
+			if constexpr (TR) {
+				tt = __shfl_sync(FULL, h1 ? o_t : t, src1);
+				pt = __shfl_sync(FULL, h2 ? o_t : t, src2);
+			}
+			o_vd = vd, o_k = k, o_vl = vl, o_t = t;
+			const int32_t e = j - 1;
+			uint64_t cv[3];
+			int32_t ck[3], ct[3] = {0, 0, 0};
+			bool keep[3] = {false, false, false}, tmp[3] = {false, false, false};
+			if (e >= 0 && e < n_a) {
+				const bool has_l = e > 0, has_r = j < n_a;
+				const bool left_in = has_l && pv == my_vd - 1, left2 = has_l && pv == my_vd - 2;
+				const bool right_in = has_r && vd == my_vd + 1, right2 = has_r && vd == my_vd + 2;
+				bool has[3];
+				// L: diagonal d-1 when absent from a: deletion from d, insertion from d-2
+				has[0] = !left_in;
+				cv[0] = my_vd - 1;
+				ck[0] = my_k + 1, ct[0] = tt;
+				if (left2 && pk > ck[0]) ck[0] = pk, ct[0] = pt;
+				// S: diagonal d: mismatch, insertion from d-1, deletion from d+1
+				has[1] = true;
+				cv[1] = my_vd;
+				ck[1] = my_k + 1, ct[1] = tt;
+				if (left_in && pk > ck[1]) ck[1] = pk, ct[1] = pt;
+				if (right_in && k + 1 > ck[1]) ck[1] = k + 1, ct[1] = t;
+				// R: diagonal d+1 when neither d+1 nor d+2 is in a: insertion from d
+				has[2] = !right_in && !right2;
+				cv[2] = my_vd + 1;
+				ck[2] = my_k, ct[2] = tt;
+				// the reference keeps vl in a uint32_t here (gwf-ed.cu:895, 993): a candidate
+				// with k = -1 (insertion before the first base of v0) fails `k < vl` and is dropped
+#pragma unroll
+				for (int q = 0; q < 3; ++q)
+					if (has[q]) {
+						const int32_t dd = vd_d(cv[q]);
+						const bool kin = rc.quirk ? (uint32_t)ck[q] < (uint32_t)my_vl : ck[q] < my_vl;
+						if (dd + ck[q] < ql && kin) keep[q] = true;
+						else if (ck[q] == my_vl) tmp[q] = true;
+					}
+			}
+			{
+				const uint32_t lt = lanemask_lt();
+				const uint32_t k0 = __ballot_sync(FULL, keep[0]), k1 = __ballot_sync(FULL, keep[1]),
+				               k2 = __ballot_sync(FULL, keep[2]);
+				int32_t off = n_x + __popc(k0 & lt) + __popc(k1 & lt) + __popc(k2 & lt);
+#pragma unroll
+				for (int q = 0; q < 3; ++q)
+					if (keep[q]) {
+						if (off < c.x) {
+							X_VD[off] = cv[q], X_K[off] = ck[q];
+							if constexpr (TR) X_T[off] = ct[q];
+						}
+						++off;
+					}
+				n_x += __popc(k0) + __popc(k1) + __popc(k2);
+				const uint32_t t0 = __ballot_sync(FULL, tmp[0]), t1 = __ballot_sync(FULL, tmp[1]),
+				               t2 = __ballot_sync(FULL, tmp[2]);
+				if (t0 | t1 | t2) {
+					int32_t offt = n_tb + __popc(t0 & lt) + __popc(t1 & lt) + __popc(t2 & lt);
+#pragma unroll
+					for (int q = 0; q < 3; ++q)
+						if (tmp[q]) {
+							if (offt < c.tb) TB[offt] = cv[q];
+							++offt;
+						}
+					n_tb += __popc(t0) + __popc(t1) + __popc(t2);
+				}
+			}
 		}
 		if (__any_sync(FULL, found)) {
 			dist = s;
@@ -268,88 +357,6 @@ __device__ __noinline__ void align_read_t(const KParams &p, int32_t r, uint8_t *
 			break;
 		}
 		if (n_e > c.w) ovf = true;
-		__syncwarp();
-
-		// ---- phase 2: in-vertex successors, sorted and unique by construction
-		// (gwf_ed_extend_batch, gwf-ed.cu:912-1016)
-		int32_t n_x = 0, n_tb = 0;
-		for (int32_t base = 0; base < n_a; base += 32) {
-			const int32_t j = base + lane;
-			uint64_t cv[3];
-			int32_t ck[3], ct[3] = {0, 0, 0};
-			bool keep[3] = {false, false, false}, tmp[3] = {false, false, false};
-			if (j < n_a) {
-				const uint64_t vd = A_VD[j];
-				const int32_t k = A_K[j];
-				int32_t tt = 0, pt = 0, nt = 0;
-				if constexpr (TR) {
-					tt = A_T[j];
-					pt = j > 0 ? A_T[j - 1] : 0;
-					nt = j + 1 < n_a ? A_T[j + 1] : 0;
-				}
-				const int32_t vl = (int32_t)__ldg(g.len + vd_v(vd));
-				const uint64_t pv = j > 0 ? A_VD[j - 1] : 0;
-				const int32_t pk = j > 0 ? A_K[j - 1] : 0;
-				const uint64_t nv = j + 1 < n_a ? A_VD[j + 1] : 0;
-				const int32_t nk = j + 1 < n_a ? A_K[j + 1] : 0;
-				const bool left_in = j > 0 && pv == vd - 1, left2 = j > 0 && pv == vd - 2;
-				const bool right_in = j + 1 < n_a && nv == vd + 1, right2 = j + 1 < n_a && nv == vd + 2;
-				bool has[3];
-				// L: diagonal d-1 when absent from a: deletion from d, insertion from d-2
-				has[0] = !left_in;
-				cv[0] = vd - 1;
-				ck[0] = k + 1, ct[0] = tt;
-				if (left2 && pk > ck[0]) ck[0] = pk, ct[0] = pt;
-				// S: diagonal d: mismatch, insertion from d-1, deletion from d+1
-				has[1] = true;
-				cv[1] = vd;
-				ck[1] = k + 1, ct[1] = tt;
-				if (left_in && pk > ck[1]) ck[1] = pk, ct[1] = pt;
-				if (right_in && nk + 1 > ck[1]) ck[1] = nk + 1, ct[1] = nt;
-				// R: diagonal d+1 when neither d+1 nor d+2 is in a: insertion from d
-				has[2] = !right_in && !right2;
-				cv[2] = vd + 1;
-				ck[2] = k, ct[2] = tt;
-				// the reference keeps vl in a uint32_t here (gwf-ed.cu:895, 993): a candidate
-				// with k = -1 (insertion before the first base of v0) fails `k < vl` and is dropped
-#pragma unroll
-				for (int t = 0; t < 3; ++t)
-					if (has[t]) {
-						const int32_t dd = vd_d(cv[t]);
-						const bool kin = rc.quirk ? (uint32_t)ck[t] < (uint32_t)vl : ck[t] < vl;
-						if (dd + ck[t] < ql && kin) keep[t] = true;
-						else if (ck[t] == vl) tmp[t] = true;
-					}
-			}
-			{
-				const uint32_t lt = lanemask_lt();
-				const uint32_t k0 = __ballot_sync(FULL, keep[0]), k1 = __ballot_sync(FULL, keep[1]),
-				               k2 = __ballot_sync(FULL, keep[2]);
-				int32_t off = n_x + __popc(k0 & lt) + __popc(k1 & lt) + __popc(k2 & lt);
-#pragma unroll
-				for (int t = 0; t < 3; ++t)
-					if (keep[t]) {
-						if (off < c.x) {
-							X_VD[off] = cv[t], X_K[off] = ck[t];
-							if constexpr (TR) X_T[off] = ct[t];
-						}
-						++off;
-					}
-				n_x += __popc(k0) + __popc(k1) + __popc(k2);
-				const uint32_t t0 = __ballot_sync(FULL, tmp[0]), t1 = __ballot_sync(FULL, tmp[1]),
-				               t2 = __ballot_sync(FULL, tmp[2]);
-				if (t0 | t1 | t2) {
-					int32_t offt = n_tb + __popc(t0 & lt) + __popc(t1 & lt) + __popc(t2 & lt);
-#pragma unroll
-					for (int t = 0; t < 3; ++t)
-						if (tmp[t]) {
-							if (offt < c.tb) TB[offt] = cv[t];
-							++offt;
-						}
-					n_tb += __popc(t0) + __popc(t1) + __popc(t2);
-				}
-			}
-		}
 		if (n_x > c.x || n_tb > c.tb) ovf = true;
 		__syncwarp();
 
