@@ -101,7 +101,8 @@ constexpr int32_t kRadixMin = 128;
 // the lag pruning of p.max_lag (a separate instantiation, so that the distance kernel's code is
 // untouched by it).
 template <bool TR, bool LAG>
-__device__ __noinline__ void align_read_t(const KParams &p, int32_t r, uint8_t *wsb, int32_t ql_cap, int32_t level)
+__device__ __forceinline__ void align_read_body(const KParams &p, int32_t r, uint8_t *wsb, int32_t ql_cap,
+                                                int32_t level)
 {
 	const int lane = threadIdx.x & 31;
 	const Caps c = caps_for(p.r.ql[r] < ql_cap ? p.r.ql[r] : ql_cap, level, p.dens_milli);
@@ -432,8 +433,11 @@ __device__ __noinline__ void align_read_t(const KParams &p, int32_t r, uint8_t *
 						if constexpr (TR) N_T[pe] = rec;
 					}
 					n_n += __popc(me);
-					int32_t tot;
-					int32_t pb = warp_excl_scan(two ? 2 : (one ? 1 : 0), &tot) + n_ba;
+					// positions in lane order: two entries per `two` lane, one per `one` lane
+					const uint32_t m2 = __ballot_sync(FULL, two), m1 = __ballot_sync(FULL, one);
+					const uint32_t lt = lanemask_lt();
+					const int32_t pb = n_ba + 2 * __popc(m2 & lt) + __popc(m1 & lt);
+					const int32_t tot = 2 * __popc(m2) + __popc(m1);
 					if (two) {
 						if (pb + 1 < c.ba) {
 							BA_VD[pb] = gen_vd(w, i - ol), BA_K[pb] = ol;         // deletion
@@ -461,11 +465,7 @@ __device__ __noinline__ void align_read_t(const KParams &p, int32_t r, uint8_t *
 				}
 				n_ba += __popc(mi);
 			}
-			{
-				int32_t tot;
-				warp_excl_scan(n_keys, &tot);
-				if (tot > hlimit) ovf = true;
-			}
+			if ((int32_t)__reduce_add_sync(FULL, (uint32_t)n_keys) > hlimit) ovf = true;
 			if (n_n > c.w || n_ba > c.ba || n_ta > c.ta) ovf = true;
 			if (TR && n_log > to.log_cap) ovf = true;
 			if (__any_sync(FULL, ovf)) {
@@ -846,6 +846,19 @@ __device__ __noinline__ void align_read_t(const KParams &p, int32_t r, uint8_t *
 #undef BK
 #undef TLOG
 
+// Out-of-line copy of the read loop, for the kernels that hold it beside other work (serving,
+// read classes, traceback). The two batch kernels below inline the body, one instantiation per
+// kernel, and run four CTAs of 8 warps per SM at 64 registers. Inlined, the body spills less at a
+// given register count (-Xptxas -v at 80 registers: 200 B stack against 264 B out of line); at 64
+// registers it spills about as much as the out-of-line body did at 80, and the 32 warps per SM
+// hide more load latency than 24 (config 3: 438 -> 416 ms; config 2: 33.6 -> 32.2 ms; config 4
+// unchanged).
+template <bool TR, bool LAG>
+__device__ __noinline__ void align_read_t(const KParams &p, int32_t r, uint8_t *wsb, int32_t ql_cap, int32_t level)
+{
+	align_read_body<TR, LAG>(p, r, wsb, ql_cap, level);
+}
+
 __device__ __forceinline__ void align_read(const KParams &p, int32_t r, uint8_t *wsb, int32_t ql_cap, int32_t level)
 {
 	if (p.max_lag > 0) align_read_t<false, true>(p, r, wsb, ql_cap, level);
@@ -853,12 +866,14 @@ __device__ __forceinline__ void align_read(const KParams &p, int32_t r, uint8_t 
 }
 
 // Plain form: one warp per queue position, arena offsets per read (main.cu:151-236 layout).
-__global__ void __launch_bounds__(256, 3) k_align_plain(const __grid_constant__ KParams p)
+// LAG = (p.max_lag > 0), chosen by the host.
+template <bool LAG>
+__global__ void __launch_bounds__(256, 4) k_align_plain(const __grid_constant__ KParams p)
 {
 	const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
 	if (gw >= p.n_order) return;
 	const int32_t r = p.order[gw];
-	align_read(p, r, p.ws + p.slot_off[gw], p.r.ql[r], p.level);
+	align_read_body<false, LAG>(p, r, p.ws + p.slot_off[gw], p.r.ql[r], p.level);
 }
 
 // Traceback form: the plain form's launch shape, arenas with the trace arrays, paths written out.
@@ -872,8 +887,9 @@ __global__ void __launch_bounds__(256, 2) k_align_trace(const __grid_constant__ 
 
 // Persistent form: each warp owns one arena (sized for ql_cap) and pulls reads from the
 // cost-ordered queue; each read uses the capacities of its own length, so a short read clears
-// and touches only the arena it needs.
-__global__ void __launch_bounds__(256, 3) k_align_persistent(const __grid_constant__ KParams p)
+// and touches only the arena it needs. LAG = (p.max_lag > 0), chosen by the host.
+template <bool LAG>
+__global__ void __launch_bounds__(256, 4) k_align_persistent(const __grid_constant__ KParams p)
 {
 	const int lane = threadIdx.x & 31;
 	const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -884,7 +900,7 @@ __global__ void __launch_bounds__(256, 3) k_align_persistent(const __grid_consta
 		qi = __shfl_sync(FULL, qi, 0);
 		if (qi >= p.n_order) break;
 		const int32_t r = p.order[qi];
-		align_read(p, r, wsb, p.ql_cap, p.level);
+		align_read_body<false, LAG>(p, r, wsb, p.ql_cap, p.level);
 	}
 }
 

@@ -337,7 +337,7 @@ Engine *gwf_engine(int dev)
 		E->mem_budget = (int64_t)(fr / 2);
 	}
 	int occ = 0;
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_align_persistent, 256, 0);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_align_persistent<false>, 256, 0);
 	E->persistent_ctas_per_sm = occ > 0 ? occ : 1;
 	occ = 0;
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_align_classes, 256, 0);
@@ -560,7 +560,8 @@ static int enqueue_persistent(Engine &E, KParams p, const PersistPlan &pl, const
 	p.slot_bytes = pl.slot;
 	p.level = level;
 	p.ql_cap = ql_cap;
-	k_align_persistent<<<pl.ctas, 32 * kWarpsPerCta, 0, E.stream>>>(p);
+	if (p.max_lag > 0) k_align_persistent<true><<<pl.ctas, 32 * kWarpsPerCta, 0, E.stream>>>(p);
+	else k_align_persistent<false><<<pl.ctas, 32 * kWarpsPerCta, 0, E.stream>>>(p);
 	CK(cudaGetLastError());
 	return 0;
 }
@@ -609,7 +610,8 @@ static int launch_plain(Engine &E, KParams p, Batch &B, int *launches)
 		p.slot_off = (const int64_t *)E.slot_off.p;
 		p.level = 0;
 		const int ctas = (p.n_order + kWarpsPerCta - 1) / kWarpsPerCta;
-		k_align_plain<<<ctas, 32 * kWarpsPerCta, 0, E.stream>>>(p);
+		if (p.max_lag > 0) k_align_plain<true><<<ctas, 32 * kWarpsPerCta, 0, E.stream>>>(p);
+		else k_align_plain<false><<<ctas, 32 * kWarpsPerCta, 0, E.stream>>>(p);
 		CK(cudaGetLastError());
 		++*launches;
 		if (end < B.n) CK(cudaStreamSynchronize(E.stream)); // arenas are reused by the next chunk
@@ -935,7 +937,8 @@ int gwf_batch_fetch(Engine &E, Batch &B, int32_t *dist, int32_t *status, int32_t
 // Launches the persistent kernel with parameters built by the caller (gwf_ed_batch_noalloc).
 cudaError_t gwf_launch_persistent(const KParams &p, int ctas, int threads, cudaStream_t s)
 {
-	k_align_persistent<<<ctas, threads, 0, s>>>(p);
+	if (p.max_lag > 0) k_align_persistent<true><<<ctas, threads, 0, s>>>(p);
+	else k_align_persistent<false><<<ctas, threads, 0, s>>>(p);
 	return cudaGetLastError();
 }
 
