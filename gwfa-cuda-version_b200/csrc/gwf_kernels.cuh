@@ -650,26 +650,73 @@ __device__ __forceinline__ void align_read_body(const KParams &p, int32_t r, uin
 				for (int32_t j = lane; j < n_ba; j += 32) BK[j] = make_int2(BA_K[j], BA_T[j]), BA_K[j] = j;
 				__syncwarp();
 			}
+			int32_t n_sort = n_ba; // candidates left to sort
+			if constexpr (!TR) {
+				// 0. before the sort, drop the arc-side candidates inside an ended interval and fold
+				// those whose diagonal is among the in-vertex candidates into that entry (of a
+				// chunk's copies of one diagonal, the one with the largest k writes; chunks go in
+				// order). Most candidates end here (config 3: ~38 per step, ~3.4 kept), so only the
+				// rest are sorted. The result is that of step 1 below on the whole list: the
+				// interval test depends on the diagonal alone, and the fold keeps the largest k.
+				int32_t n_s = 0;
+				for (int32_t base = 0; base < n_ba; base += 32) {
+					const int32_t j = base + lane;
+					uint64_t vd = 0;
+					int32_t k = 0, px = 0;
+					bool fold = false, keep = false;
+					if (j < n_ba) {
+						vd = BA_VD[j], k = BA_K[j];
+						if (!in_ranges(ILO, IHI, n_i, vd, i_min, i_max)) {
+							px = upper_bound_u64(X_VD, n_x, vd);
+							fold = px > 0 && X_VD[px - 1] == vd;
+							keep = !fold;
+						}
+					}
+					// ~lane is no diagonal (its vertex part would be 2^32 - 1)
+					const uint32_t same = __match_any_sync(FULL, fold ? vd : ~(uint64_t)lane);
+					uint32_t rest = fold ? same & ~(1u << lane) : 0u;
+					bool lead = fold;
+					while (__any_sync(FULL, rest != 0)) { // at most 31 rounds, one per copy
+						const int q = rest ? __ffs(rest) - 1 : lane;
+						const int32_t kq = __shfl_sync(FULL, k, q);
+						if (rest) {
+							if (kq > k || (kq == k && q < lane)) lead = false;
+							rest &= rest - 1;
+						}
+					}
+					if (lead && k > X_K[px - 1]) X_K[px - 1] = k;
+					const uint32_t m = __ballot_sync(FULL, keep);
+					__syncwarp(); // the chunk's loads before the in-place writes
+					if (keep) {
+						const int32_t pos = n_s + __popc(m & lanemask_lt());
+						BA_VD[pos] = vd, BA_K[pos] = k;
+					}
+					n_s += __popc(m);
+					__syncwarp();
+				}
+				n_sort = n_s;
+			}
 			// the wavefront buffer a is free until this step's merge writes it: sort scratch
-			if (n_ba <= kRadixMin || !warp_radix_sort(BA_VD, BA_K, n_ba, A_VD, A_K, radix_hist))
-				warp_bitonic_sort(BA_VD, BA_K, n_ba);
+			if (n_sort <= kRadixMin || !warp_radix_sort(BA_VD, BA_K, n_sort, A_VD, A_K, radix_hist))
+				warp_bitonic_sort(BA_VD, BA_K, n_sort);
 			// 1. arc-side candidates: one per diagonal with the furthest k, minus those inside an
 			// ended interval; a diagonal also present among the in-vertex candidates folds its k
-			// into that entry (each in-vertex entry receives at most one, as the list is unique)
+			// into that entry (each in-vertex entry receives at most one, as the list is unique).
+			// Without TR, step 0 did the interval test and the fold already.
 			int32_t n_b = 0;
-			for (int32_t base = 0; base < n_ba; base += 32) {
+			for (int32_t base = 0; base < n_sort; base += 32) {
 				const int32_t j = base + lane;
 				bool keep = false;
 				uint64_t vd = 0;
 				int32_t k = 0, tk = 0;
-				if (j < n_ba) {
+				if (j < n_sort) {
 					vd = BA_VD[j], k = BA_K[j];
 					if constexpr (TR) {
 						const int2 e = BK[k];
 						k = e.x, tk = e.y;
 					}
 					if (j == 0 || BA_VD[j - 1] != vd) {
-						for (int32_t t = j + 1; t < n_ba && BA_VD[t] == vd; ++t) {
+						for (int32_t t = j + 1; t < n_sort && BA_VD[t] == vd; ++t) {
 							if constexpr (TR) {
 								const int2 e = BK[BA_K[t]];
 								if (e.x > k) k = e.x, tk = e.y;
@@ -678,17 +725,17 @@ __device__ __forceinline__ void align_read_body(const KParams &p, int32_t r, uin
 								k = kt > k ? kt : k;
 							}
 						}
-						keep = !in_ranges(ILO, IHI, n_i, vd, i_min, i_max);
-						if (keep) {
-							const int32_t px = upper_bound_u64(X_VD, n_x, vd);
-							if (px > 0 && X_VD[px - 1] == vd) {
-								if (k > X_K[px - 1]) {
-									X_K[px - 1] = k;
-									if constexpr (TR) X_T[px - 1] = tk;
+						if constexpr (TR) {
+							keep = !in_ranges(ILO, IHI, n_i, vd, i_min, i_max);
+							if (keep) {
+								const int32_t px = upper_bound_u64(X_VD, n_x, vd);
+								if (px > 0 && X_VD[px - 1] == vd) {
+									if (k > X_K[px - 1]) X_K[px - 1] = k, X_T[px - 1] = tk;
+									keep = false;
 								}
-								keep = false;
 							}
-						}
+						} else
+							keep = true;
 					}
 				}
 				__syncwarp();
