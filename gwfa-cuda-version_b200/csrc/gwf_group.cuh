@@ -740,10 +740,11 @@ __device__ __noinline__ void align_read_grp(const KParams &p, int32_t r, uint8_t
 			off_a_vd = off_x_vd, off_a_k = off_x_k, off_x_vd = tv, off_x_k = tk;
 			G.sync();
 		} else {
-			grp_sort<NW>(G, BA_VD, BA_K, n_ba, A_VD, A_K, radix_hist, hist_fits);
-			// 1. arc-side candidates: furthest k per diagonal, outside the intervals, folded into
-			// an equal in-vertex candidate where there is one
-			int32_t n_b = 0;
+			// 0. before the sort, drop the arc-side candidates inside an ended interval and fold
+			// those on an in-vertex diagonal into that entry, as align_read_t does; copies of one
+			// diagonal can sit in different warps of the group, so the fold is an atomic max, which
+			// the group barriers order before step 2 reads the in-vertex candidates
+			int32_t n_s = 0;
 			for (int32_t base = 0; base < n_ba; base += GS) {
 				const int32_t j = base + rank;
 				bool keep = false;
@@ -751,19 +752,37 @@ __device__ __noinline__ void align_read_grp(const KParams &p, int32_t r, uint8_t
 				int32_t k = 0;
 				if (j < n_ba) {
 					vd = BA_VD[j], k = BA_K[j];
+					if (!in_ranges(ILO, IHI, n_i, vd, i_min, i_max)) {
+						const int32_t px = upper_bound_u64(X_VD, n_x, vd);
+						if (px > 0 && X_VD[px - 1] == vd) atomicMax(&X_K[px - 1], k);
+						else keep = true;
+					}
+				}
+				uint32_t tot;
+				const uint32_t pre = G.scan1(keep, &tot); // a barrier: the chunk's loads come first
+				if (keep) {
+					const int32_t pos = n_s + (int32_t)pre;
+					BA_VD[pos] = vd, BA_K[pos] = k;
+				}
+				n_s += (int32_t)tot;
+			}
+			G.sync();
+			grp_sort<NW>(G, BA_VD, BA_K, n_s, A_VD, A_K, radix_hist, hist_fits);
+			// 1. the surviving arc-side candidates: furthest k per diagonal
+			int32_t n_b = 0;
+			for (int32_t base = 0; base < n_s; base += GS) {
+				const int32_t j = base + rank;
+				bool keep = false;
+				uint64_t vd = 0;
+				int32_t k = 0;
+				if (j < n_s) {
+					vd = BA_VD[j], k = BA_K[j];
 					if (j == 0 || BA_VD[j - 1] != vd) {
-						for (int32_t t = j + 1; t < n_ba && BA_VD[t] == vd; ++t) {
+						for (int32_t t = j + 1; t < n_s && BA_VD[t] == vd; ++t) {
 							const int32_t kt = BA_K[t];
 							k = kt > k ? kt : k;
 						}
-						keep = !in_ranges(ILO, IHI, n_i, vd, i_min, i_max);
-						if (keep) {
-							const int32_t px = upper_bound_u64(X_VD, n_x, vd);
-							if (px > 0 && X_VD[px - 1] == vd) {
-								if (k > X_K[px - 1]) X_K[px - 1] = k;
-								keep = false;
-							}
-						}
+						keep = true;
 					}
 				}
 				uint32_t tot;
