@@ -460,6 +460,8 @@ __device__ __noinline__ void align_read_grp(const KParams &p, int32_t r, uint8_t
 						if (dd + ck[t] < ql && kin) keep[t] = true;
 						else if (ck[t] == vl) tmp[t] = true;
 					}
+				// as in align_read_t: the first wave records this diagonal's end already
+				if (tmp[1] && k == vl - 1 && vd_d(vd) + k != ql - 1) tmp[1] = false;
 			}
 			const uint32_t kc = (uint32_t)keep[0] + keep[1] + keep[2], tc = (uint32_t)tmp[0] + tmp[1] + tmp[2];
 			uint32_t tot;

@@ -318,6 +318,10 @@ __device__ __forceinline__ void align_read_body(const KParams &p, int32_t r, uin
 						if (dd + ck[q] < ql && kin) keep[q] = true;
 						else if (ck[q] == my_vl) tmp[q] = true;
 					}
+				// a diagonal that ended its vertex short of the query end is a vertex-end state
+				// of the first wave, which records it as an ended point already: its own
+				// successor at k == vl would repeat that point
+				if (tmp[1] && my_k == my_vl - 1 && vd_d(my_vd) + my_k != ql - 1) tmp[1] = false;
 			}
 			{
 				const uint32_t lt = lanemask_lt();
