@@ -554,7 +554,8 @@ __device__ __noinline__ void align_read_grp(const KParams &p, int32_t r, uint8_t
 						else o_l = true;
 					}
 				}
-				const bool ins = isv && (nv == 0 || n_ext != nv);
+				// (first wave: phase 2 covers diagonal d + 1 already, as in align_read_t)
+				const bool ins = isv && wave > 0 && (nv == 0 || n_ext != nv);
 				const bool qdel = isq && k + 1 < vl;
 				const uint32_t pi = G.append1(ins || qdel, C_BA) - uBA;
 				if (ins || qdel) {

@@ -457,8 +457,11 @@ __device__ __forceinline__ void align_read_body(const KParams &p, int32_t r, uin
 					n_ba += tot;
 				}
 				// insertion at the vertex end (gwf-ed.cu:1225-1226); v1 >= 0 query-end deletion
-				// inside the vertex (gwf-ed.cu:1237-1241)
-				const bool ins = isv && (nv == 0 || n_ext != nv);
+				// inside the vertex (gwf-ed.cu:1237-1241). In the first wave the state is a
+				// wavefront diagonal d, and phase 2 has already given diagonal d + 1 an in-vertex
+				// candidate with k >= vl - 1 or an ended point, which the insertion (d + 1,
+				// vl - 1) could only repeat; only entered states (later waves) need it.
+				const bool ins = isv && wave > 0 && (nv == 0 || n_ext != nv);
 				const bool qdel = isq && k + 1 < vl;
 				const uint32_t mi = __ballot_sync(FULL, ins || qdel);
 				const int32_t pi = n_ba + __popc(mi & lanemask_lt());
