@@ -657,7 +657,12 @@ static int32_t share_nw(double cost, double share)
 // accessed at random): 6,000 reads of 0.5-20 kbp on the 5 Mbp graph align at 1,368 reads/s with
 // one warp per read (120 GB of arenas, cut to the memory budget) and 3,161 with eight. A read
 // whose one-warp arenas over every slot would pass that gets enough warps per read to stay below.
+// The rule applies to batches of fewer than kArenaRuleReadsPerSlot reads per warp slot, where the
+// longest reads set the batch's end; with more, the queue keeps every warp busy and one warp per
+// read is the faster shape (20,000 reads of 10 kbp on the 5 Mbp graph, 4.2 per slot: 8,046 reads/s
+// with one warp per read against 6,858 with the four that the rule gave them).
 static const double kLiveArenaBytes = 16.0 * (1LL << 30);
+static const double kArenaRuleReadsPerSlot = 3.0;
 
 static int32_t arena_nw(int32_t ql, int32_t dens_milli, int64_t slots)
 {
@@ -693,8 +698,9 @@ static int plan_classes(Engine &E, Batch &B, const int32_t *nw_b, int64_t slots,
 	double total = 0;
 	for (int32_t i = 0; i < B.n; ++i) total += (double)B.h_ql[(size_t)i] * (double)B.h_ql[(size_t)i];
 	const double share = total / (double)std::max<int64_t>(1, slots);
-	int32_t from[3];
-	arena_nw_lengths(B.max_ql, dens_milli, slots, from);
+	int32_t from[3] = {INT32_MAX, INT32_MAX, INT32_MAX}; // lengths from which the arena rule gives 2, 4, 8
+	if ((double)B.n < kArenaRuleReadsPerSlot * (double)std::max<int64_t>(1, slots))
+		arena_nw_lengths(B.max_ql, dens_milli, slots, from);
 	int32_t cnt[4] = {0, 0, 0, 0}, cap[4] = {0, 0, 0, 0};
 	std::vector<uint8_t> cls((size_t)B.n);
 	for (int32_t i = 0; i < B.n; ++i) {

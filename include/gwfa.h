@@ -86,8 +86,9 @@ typedef struct {
 	                           0 = per read: the gwf_tune value of its length bucket for
 	                           GWF_MODE_AUTO, else by its share of the batch's work (cost ql^2
 	                           against the persistent grid's warp slots) and by its arena size:
-	                           reads costing more than one slot's even share, or whose arenas over
-	                           every slot would pass 16 GiB, get 2, 4 or 8 warps, the others one.
+	                           reads costing more than one slot's even share, or (in batches of
+	                           fewer than 3 reads per warp slot) whose arenas over every slot
+	                           would pass 16 GiB, get 2, 4 or 8 warps, the others one.
 	                           The plain form uses one warp per read. */
 	int32_t ctas_per_sm;   /* persistent grid; 0 = the autotuned value for GWF_MODE_AUTO (see
 	                          gwf_tune), else the occupancy limit */
