@@ -662,7 +662,7 @@ __device__ __forceinline__ void align_read_body(const KParams &p, int32_t r, uin
 				// 0. before the sort, drop the arc-side candidates inside an ended interval and fold
 				// those whose diagonal is among the in-vertex candidates into that entry (of a
 				// chunk's copies of one diagonal, the one with the largest k writes; chunks go in
-				// order). Most candidates end here (config 3: ~38 per step, ~3.4 kept), so only the
+				// order). Most candidates end here (config 3: ~27 per step, ~4.4 left), so only the
 				// rest are sorted. The result is that of step 1 below on the whole list: the
 				// interval test depends on the diagonal alone, and the fold keeps the largest k.
 				int32_t n_s = 0;
